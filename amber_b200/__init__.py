@@ -1,0 +1,280 @@
+"""amber_b200 — B200-native AMBER estimator hot path.
+
+The product is ``libamber_cuda.so`` (hand-written sm_100a CUDA behind the C
+ABI of ``include/amber_cuda.h``).  This module loads it with ctypes and
+mirrors the reference's own call sequence (4_fbe/amber.c:40-304):
+
+    est = Estimator(precision="mixed")          # or "fp64": the plain path
+    est.load_grid(gv_sums, counts, Du, flag_key) # initialize + ReadGVnAC_gridding + normalize_data
+    est.set_rings(ULow, UHigh)                   # annular_rings
+    est.set_channels(nc10, uf_chans)             # get_uf_chans + vcp table
+    rdata = est.calcr()                          # calCR + read_rings
+    Ntri, Num, bldnu, numdnu = est.triangle_v1(r1, r2, r3, rdata[rp, 3])
+    inv, bldnu, numdnu = est.triangle_v2(r1, r2, r3)
+
+There is no CPU fallback: without the library or without an sm_100 GPU every
+call raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libamber_cuda.so")
+
+AMBER_OK = 0
+ERRORS = {-1: "bad argument", -2: "out of device memory / over budget", -3: "CUDA error", -4: "timeout",
+          -5: "overflow", -6: "call order", -7: "no sm_100 device"}
+PREC = {"fp64": 0, "mixed": 1}
+
+# every entry point include/amber_cuda.h declares
+EXPORTS = (
+    "amber_cuda_default_opts", "amber_cuda_create", "amber_cuda_destroy", "amber_cuda_last_error",
+    "amber_cuda_load_grid_packed", "amber_cuda_load_grid", "amber_cuda_set_rings", "amber_cuda_get_uavg",
+    "amber_cuda_set_channels", "amber_cuda_calcr", "amber_cuda_ng1", "amber_cuda_triangle_v1",
+    "amber_cuda_triangle_v2", "amber_cuda_triangles", "amber_cuda_triangles_run", "amber_cuda_triangles_fetch",
+    "amber_cuda_last_run_stats", "amber_cuda_grid_vis",
+)
+
+
+class AmberError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"libamber_cuda error {code} ({ERRORS.get(code, '?')}): {msg}")
+        self.code = code
+
+
+class Opts(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("precision", ctypes.c_int), ("hbm_budget", ctypes.c_size_t),
+                ("stream", ctypes.c_void_p), ("chunk_px", ctypes.c_int)]
+
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_fp = ctypes.POINTER(ctypes.c_float)
+_ip = ctypes.POINTER(ctypes.c_int)
+_i32p = ctypes.POINTER(ctypes.c_int32)
+_i64p = ctypes.POINTER(ctypes.c_int64)
+_vp = ctypes.c_void_p
+_lib = None
+
+
+def load_library():
+    """Load libamber_cuda.so (raises if it has not been built: no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `python -m amber_b200.build` "
+                          "(there is no CPU fallback)")
+    L = ctypes.CDLL(LIB_PATH)
+    L.amber_cuda_default_opts.argtypes = [ctypes.POINTER(Opts)]
+    L.amber_cuda_create.argtypes = [ctypes.POINTER(Opts), ctypes.POINTER(_vp)]
+    L.amber_cuda_destroy.argtypes = [_vp]
+    L.amber_cuda_destroy.restype = None
+    L.amber_cuda_last_error.argtypes = [_vp]
+    L.amber_cuda_last_error.restype = ctypes.c_char_p
+    L.amber_cuda_load_grid_packed.argtypes = [_vp, ctypes.c_long, ctypes.c_long, ctypes.c_double, ctypes.c_int, _dp,
+                                              _dp]
+    L.amber_cuda_load_grid.argtypes = [_vp, ctypes.c_long, ctypes.c_long, ctypes.c_double, ctypes.c_int,
+                                       ctypes.POINTER(_dp), ctypes.POINTER(_dp), ctypes.POINTER(_dp)]
+    L.amber_cuda_set_rings.argtypes = [_vp, ctypes.c_int, _dp, _dp]
+    L.amber_cuda_get_uavg.argtypes = [_vp, _dp]
+    L.amber_cuda_set_channels.argtypes = [_vp, ctypes.c_int, ctypes.c_int, _ip]
+    L.amber_cuda_calcr.argtypes = [_vp, ctypes.c_int, _ip, _dp]
+    L.amber_cuda_ng1.argtypes = [_vp, ctypes.c_int]
+    L.amber_cuda_ng1.restype = ctypes.c_long
+    L.amber_cuda_triangle_v1.argtypes = [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, _fp, _i32p,
+                                         _dp, _dp]
+    L.amber_cuda_triangle_v2.argtypes = [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _fp, _fp, _dp]
+    L.amber_cuda_triangles.argtypes = [_vp, ctypes.c_int, _ip, ctypes.c_int, _dp, _i64p, _dp]
+    L.amber_cuda_triangles_run.argtypes = [_vp, ctypes.c_int, _ip, ctypes.c_int]
+    L.amber_cuda_triangles_fetch.argtypes = [_vp, _dp, _i64p, _dp]
+    L.amber_cuda_last_run_stats.argtypes = [_vp, _dp, _dp]
+    L.amber_cuda_grid_vis.argtypes = [_vp, ctypes.c_long, ctypes.c_long, ctypes.c_double, ctypes.c_double,
+                                      ctypes.c_float, ctypes.c_int, ctypes.c_long, ctypes.c_long, ctypes.c_long, _fp,
+                                      _fp, _dp, _dp]
+    _lib = L
+    return L
+
+
+def _ptr(a, t):
+    return None if a is None else a.ctypes.data_as(t)
+
+
+class Estimator:
+    """One libamber_cuda context (one device, one host thread)."""
+
+    def __init__(self, device: int = 0, precision: str = "mixed", hbm_budget: int = 0, stream: int | None = None,
+                 chunk_px: int = 0):
+        self._L = load_library()
+        o = Opts(device, PREC[precision], hbm_budget, stream or None, chunk_px)
+        h = _vp()
+        rc = self._L.amber_cuda_create(ctypes.byref(o), ctypes.byref(h))
+        if rc != AMBER_OK:
+            raise AmberError(rc, "amber_cuda_create failed (an sm_100 GPU is required)")
+        self._h = h
+        self.precision = precision
+        self.nc10 = None
+        self.n1 = None
+        self.nc = None
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.amber_cuda_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, rc):
+        if rc != AMBER_OK:
+            raise AmberError(rc, self._L.amber_cuda_last_error(self._h).decode(errors="replace"))
+
+    # ---- inputs -----------------------------------------------------------
+    def load_grid(self, gv_sums: np.ndarray, counts: np.ndarray, du: float, flag_key: int):
+        """Upload summed visibilities (complex [NN, NN/2+1, nc]) and counts; normalised on the device."""
+        nn, h, nc = gv_sums.shape
+        ri = np.ascontiguousarray(gv_sums, dtype=np.complex128).view(np.float64)
+        nt = np.ascontiguousarray(counts, dtype=np.float64)
+        self._check(self._L.amber_cuda_load_grid_packed(self._h, nn, nc, float(du), int(flag_key), _ptr(ri, _dp),
+                                                        _ptr(nt, _dp)))
+        self.n1, self.nc = nn, nc
+
+    def load_grid_raw(self, re_im_ptr: int, ntig_ptr: int, nn: int, nc: int, du: float, flag_key: int):
+        """Same as load_grid but from raw host addresses (e.g. pinned buffers)."""
+        self._check(self._L.amber_cuda_load_grid_packed(self._h, nn, nc, float(du), int(flag_key),
+                                                        ctypes.cast(re_im_ptr, _dp), ctypes.cast(ntig_ptr, _dp)))
+        self.n1, self.nc = nn, nc
+
+    def load_grid_cells(self, gv_sums, counts, du, flag_key):
+        """Pointer-per-cell form (the reference's double** arrays)."""
+        nn, h, nc = gv_sums.shape
+        ncell = nn * h
+        re = np.ascontiguousarray(gv_sums.real.reshape(ncell, nc))
+        im = np.ascontiguousarray(gv_sums.imag.reshape(ncell, nc))
+        nt = np.ascontiguousarray(counts.reshape(ncell, nc), dtype=np.float64)
+        mk = lambda a: (_dp * ncell)(*[a[i].ctypes.data_as(_dp) for i in range(ncell)])
+        self._check(self._L.amber_cuda_load_grid(self._h, nn, nc, float(du), int(flag_key), mk(re), mk(im), mk(nt)))
+        self.n1, self.nc = nn, nc
+
+    def set_rings(self, ulow, uhigh):
+        lo = np.ascontiguousarray(ulow, dtype=np.float64)
+        hi = np.ascontiguousarray(uhigh, dtype=np.float64)
+        self._check(self._L.amber_cuda_set_rings(self._h, len(lo), _ptr(lo, _dp), _ptr(hi, _dp)))
+        self.nr = len(lo)
+
+    def uavg(self):
+        out = np.zeros(self.nr)
+        self._check(self._L.amber_cuda_get_uavg(self._h, _ptr(out, _dp)))
+        return out
+
+    def set_channels(self, nc10: int, uf_chans=None):
+        uf = None if uf_chans is None else np.ascontiguousarray(uf_chans, dtype=np.int32)
+        self._check(self._L.amber_cuda_set_channels(self._h, int(nc10), 0 if uf is None else len(uf),
+                                                    _ptr(uf, _ip)))
+        self.nc10 = int(nc10)
+
+    # ---- estimator --------------------------------------------------------
+    def calcr(self) -> np.ndarray:
+        n = ctypes.c_int(0)
+        self._check(self._L.amber_cuda_calcr(self._h, 0, ctypes.byref(n), None))
+        out = np.zeros((max(n.value, 1), 4))
+        self._check(self._L.amber_cuda_calcr(self._h, n.value, ctypes.byref(n), _ptr(out, _dp)))
+        return out[: n.value]
+
+    def ng1(self, r1: int) -> int:
+        return int(self._L.amber_cuda_ng1(self._h, int(r1)))
+
+    @property
+    def nclen(self):
+        return 2 * self.nc10 + 1
+
+    def triangle_v1(self, r1, r2, r3, rdata_num):
+        n = self.nclen
+        bl = np.zeros((n, n), dtype=np.float32)
+        nd = np.zeros((n, n), dtype=np.int32)
+        ntri, num = ctypes.c_double(), ctypes.c_double()
+        self._check(self._L.amber_cuda_triangle_v1(self._h, r1, r2, r3, float(rdata_num), _ptr(bl, _fp),
+                                                   _ptr(nd, _i32p), ctypes.byref(ntri), ctypes.byref(num)))
+        return ntri.value, num.value, bl, nd
+
+    def triangle_v2(self, r1, r2, r3):
+        n = self.nclen
+        bl = np.zeros((n, n), dtype=np.float32)
+        nd = np.zeros((n, n), dtype=np.float32)
+        inv = ctypes.c_double()
+        self._check(self._L.amber_cuda_triangle_v2(self._h, r1, r2, r3, _ptr(bl, _fp), _ptr(nd, _fp),
+                                                   ctypes.byref(inv)))
+        return inv.value, bl, nd
+
+    def run(self, tri, want_v2=False):
+        tri = np.ascontiguousarray(np.asarray(tri, dtype=np.int32).reshape(-1, 3))
+        self._ntri = len(tri)
+        self._check(self._L.amber_cuda_triangles_run(self._h, len(tri), _ptr(tri, _ip), int(bool(want_v2))))
+
+    def fetch(self, want_v2=False):
+        n = self.nclen
+        bl = np.zeros((self._ntri, n, n))
+        nd = np.zeros((self._ntri, n, n), dtype=np.int64)
+        nt = np.zeros((self._ntri, n, n)) if want_v2 else None
+        self._check(self._L.amber_cuda_triangles_fetch(self._h, _ptr(bl, _dp), _ptr(nd, _i64p), _ptr(nt, _dp)))
+        return bl, nd, nt
+
+    def triangles(self, tri, want_v2=False):
+        """FP64 lag arrays for many triangles: (bldnu, numdnu int64, numtri or None)."""
+        self.run(tri, want_v2)
+        return self.fetch(want_v2)
+
+    def last_run_stats(self):
+        p, ms = ctypes.c_double(), ctypes.c_double()
+        self._check(self._L.amber_cuda_last_run_stats(self._h, ctypes.byref(p), ctypes.byref(ms)))
+        return p.value, ms.value
+
+    # ---- gridding ---------------------------------------------------------
+    def grid_vis(self, nn, nc, du, umax, nu_chan0, flag_key, randpar, data):
+        randpar = np.ascontiguousarray(randpar, dtype=np.float32)
+        data = np.ascontiguousarray(data, dtype=np.float32)
+        g, npar = randpar.shape
+        nstokes = data.shape[2]
+        h = nn // 2 + 1
+        ri = np.zeros((nn, h, nc, 2))
+        nt = np.zeros((nn, h, nc))
+        self._check(self._L.amber_cuda_grid_vis(self._h, nn, nc, float(du), float(umax), np.float32(nu_chan0),
+                                                int(flag_key), g, npar, nstokes, _ptr(randpar, _fp), _ptr(data, _fp),
+                                                _ptr(ri, _dp), _ptr(nt, _dp)))
+        return ri[..., 0] + 1j * ri[..., 1], nt
+
+
+def estimate(real, precision="mixed", version=1, tri_subset=None, est: Estimator | None = None):
+    """Run the whole estimator on a synth.Realisation; returns (rdata, results)
+    where results[i] = dict(r1, r2, r3, bldnu (FP64), numdnu (int64), numtri)."""
+    own = est is None
+    est = est or Estimator(precision=precision)
+    try:
+        est.load_grid(real.gv, real.counts, real.du, real.flag_key)
+        est.set_rings(real.ulow, real.uhigh)
+        est.set_channels(real.nc10, real.uf_chans if real.flag_key == 1 else None)
+        rdata = est.calcr()
+        idx = list(range(len(rdata))) if tri_subset is None else list(tri_subset)
+        tri = rdata[idx, :3].astype(np.int32)
+        bl, nd, nt = est.triangles(tri, want_v2=(version == 2))
+        out = []
+        for i, t in enumerate(idx):
+            out.append(dict(rp=t, r1=int(tri[i, 0]), r2=int(tri[i, 1]), r3=int(tri[i, 2]), ng1=est.ng1(int(tri[i, 0])),
+                            rdata_num=float(rdata[t, 3]), bldnu=bl[i], numdnu=nd[i],
+                            numtri=None if nt is None else nt[i]))
+        return rdata, out
+    finally:
+        if own:
+            est.close()

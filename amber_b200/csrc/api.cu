@@ -1,0 +1,632 @@
+// extern "C" entry points of libamber_cuda (declared in include/amber_cuda.h)
+// and the host-side control flow that replaces the rp loop of 4_fbe/amber.c /
+// amber_v2.c: grid upload + normalisation, ring geometry, calCR, closed-form
+// triplet counts, and per-r1-group map building followed by the per-triangle
+// contraction.
+#include <math.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <set>
+#include <vector>
+
+#include "common.cuh"
+
+namespace amber {
+
+int fail(amber_cuda_ctx *c, int code, const char *fmt, ...)
+{
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    if (c) c->err = buf;
+    return code;
+}
+
+int cuda_check(amber_cuda_ctx *c, cudaError_t e, const char *what)
+{
+    if (e == cudaSuccess) return AMBER_OK;
+    return fail(c, e == cudaErrorMemoryAllocation ? AMBER_ERR_OOM : AMBER_ERR_CUDA, "%s: %s", what,
+                cudaGetErrorString(e));
+}
+
+int ensure(amber_cuda_ctx *c, DevBuf &b, size_t bytes, const char *what)
+{
+    if (bytes <= b.bytes) return AMBER_OK;
+    size_t want = std::max(bytes, b.bytes + b.bytes / 4);
+    if (c->held - b.bytes + want > c->budget) {
+        want = bytes;
+        if (c->held - b.bytes + want > c->budget)
+            return fail(c, AMBER_ERR_OOM, "%s: %zu bytes would exceed the HBM budget (%zu held of %zu)", what, bytes,
+                        c->held, c->budget);
+    }
+    if (b.p) {
+        cudaStreamSynchronize(c->stream);
+        cudaFree(b.p);
+        c->held -= b.bytes;
+        b.p = nullptr;
+        b.bytes = 0;
+    }
+    cudaError_t e = cudaMalloc(&b.p, want);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(c, AMBER_ERR_OOM, "%s: cudaMalloc(%zu) failed: %s", what, want, cudaGetErrorString(e));
+    }
+    b.bytes = want;
+    c->held += want;
+    return AMBER_OK;
+}
+
+static void release(amber_cuda_ctx *c, DevBuf &b)
+{
+    if (b.p) {
+        cudaFree(b.p);
+        c->held -= b.bytes;
+    }
+    b.p = nullptr;
+    b.bytes = 0;
+}
+
+int twiddle_table(amber_cuda_ctx *c, long n, const double2 **out)
+{
+    auto it = c->twiddles.find(n);
+    if (it == c->twiddles.end()) {
+        std::vector<double2> h(n);
+        for (long k = 0; k < n; ++k) {
+            long double a = 2.0L * 3.14159265358979323846264338327950288L * (long double)k / (long double)n;
+            h[k] = make_double2((double)cosl(a), (double)sinl(a));
+        }
+        DevBuf b;
+        int rc = ensure(c, b, sizeof(double2) * n, "twiddle table");
+        if (rc) return rc;
+        rc = cuda_check(c, cudaMemcpy(b.p, h.data(), sizeof(double2) * n, cudaMemcpyHostToDevice), "twiddles");
+        if (rc) return rc;
+        it = c->twiddles.emplace(n, b).first;
+    }
+    *out = reinterpret_cast<const double2 *>(it->second.p);
+    return AMBER_OK;
+}
+
+namespace {
+
+// normalize_data (amber_funcs.c:1946-1978): GV /= NTiG where NTiG > 0, then
+// NTiG := 1 there (it becomes the 0/1 sampling mask).
+__global__ void normalize_kernel(const double2 *__restrict__ sums, const double *__restrict__ counts, long n,
+                                 double2 *__restrict__ grid, double *__restrict__ mask)
+{
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        double2 v = sums[i];
+        double t = counts[i];
+        if (t > 0) {
+            v.x /= t;
+            v.y /= t;
+            t = 1;
+        }
+        grid[i] = v;
+        mask[i] = t;
+    }
+}
+
+long ng1_of(double uhigh, double du)
+{
+    // amber.c:193-197
+    double umax = uhigh + 3;
+    long nmax = (long)(umax / du);
+    long ng = (long)(3 * nmax);
+    return (ng % 2 == 0) ? ng + 2 : ng + 3;
+}
+
+bool closed(const std::vector<double> &ua, int r1, int r2, int r3)
+{
+    // calCR's rule, amber_funcs.c:439-449
+    double tt = ua[r2] / ua[r1];
+    if (!(tt >= 0.5 && tt <= 1.0)) return false;
+    double mu = 0.5 * (tt + 1. / tt - (ua[r3] / ua[r1]) * (ua[r3] / ua[r2]));
+    return mu >= 0.5 / tt && mu <= 1.0;
+}
+
+int check_ready(amber_cuda_ctx *c, bool need_channels)
+{
+    if (!c->grid.p) return fail(c, AMBER_ERR_STATE, "no grid loaded");
+    if (c->Nr <= 0) return fail(c, AMBER_ERR_STATE, "no rings set");
+    for (int r = 0; r < c->Nr; ++r)
+        if (c->uhigh[r] > c->N1 / 2)
+            return fail(c, AMBER_ERR_ARG, "ring %d reaches U=%g beyond the grid half-width %ld", r, c->uhigh[r],
+                        c->N1 / 2);
+    if (need_channels && c->nc10 < 0) return fail(c, AMBER_ERR_STATE, "no channels set");
+    if (need_channels && (long)c->weight.size() != c->nc)
+        return fail(c, AMBER_ERR_STATE, "channels were set for a different channel count");
+    return AMBER_OK;
+}
+
+int upload_grid(amber_cuda_ctx *c, long N1, long nc, double Du, int flag_key, const double *re_im,
+                const double *ntig)
+{
+    if (N1 <= 0 || N1 % 2 || nc <= 0 || !(Du > 0) || !re_im || !ntig)
+        return fail(c, AMBER_ERR_ARG, "bad grid arguments (N1=%ld nc=%ld Du=%g)", N1, nc, Du);
+    if (flag_key != 0 && flag_key != 1) return fail(c, AMBER_ERR_ARG, "flag_key must be 0 or 1 (got %d)", flag_key);
+    const long n = N1 * (N1 / 2 + 1) * nc;
+    int rc;
+    if ((rc = ensure(c, c->grid, sizeof(double2) * n, "grid"))) return rc;
+    if ((rc = ensure(c, c->mask, sizeof(double) * n, "sampling mask"))) return rc;
+    // the raw sums land in the partial buffer first, then normalise into grid/mask
+    if ((rc = ensure(c, c->partial, sizeof(double2) * n + sizeof(double) * n, "grid staging"))) return rc;
+    double2 *raw = (double2 *)c->partial.p;
+    double *cnt = (double *)((char *)c->partial.p + sizeof(double2) * n);
+    if ((rc = cuda_check(c, cudaMemcpyAsync(raw, re_im, sizeof(double2) * n, cudaMemcpyHostToDevice, c->stream),
+                         "upload grid")))
+        return rc;
+    if ((rc = cuda_check(c, cudaMemcpyAsync(cnt, ntig, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream),
+                         "upload sampling")))
+        return rc;
+    normalize_kernel<<<4 * c->num_sms, 256, 0, c->stream>>>(raw, cnt, n, (double2 *)c->grid.p, (double *)c->mask.p);
+    if ((rc = cuda_check(c, cudaGetLastError(), "normalize launch"))) return rc;
+    c->N1 = N1;
+    c->nc = nc;
+    c->Du = Du;
+    c->flag_key = flag_key;
+    return cuda_check(c, cudaStreamSynchronize(c->stream), "grid upload");
+}
+
+// Which rings each r1 group needs, for a list of triangles.
+struct Group {
+    int r1;
+    long ng;
+    std::vector<int> tris;  // indices into the caller's list
+};
+
+}  // namespace
+}  // namespace amber
+
+using namespace amber;
+
+extern "C" {
+
+void amber_cuda_default_opts(amber_cuda_opts *o)
+{
+    if (!o) return;
+    memset(o, 0, sizeof(*o));
+    o->precision = AMBER_PREC_MIXED;
+}
+
+int amber_cuda_create(const amber_cuda_opts *opts, amber_cuda_ctx **out)
+{
+    if (!out) return AMBER_ERR_ARG;
+    *out = nullptr;
+    amber_cuda_opts o;
+    amber_cuda_default_opts(&o);
+    if (opts) o = *opts;
+    if (o.precision != AMBER_PREC_FP64 && o.precision != AMBER_PREC_MIXED) return AMBER_ERR_ARG;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= o.device) {
+        cudaGetLastError();
+        return AMBER_ERR_NODEV;
+    }
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, o.device) != cudaSuccess || prop.major != 10) return AMBER_ERR_NODEV;
+    if (cudaSetDevice(o.device) != cudaSuccess) return AMBER_ERR_NODEV;
+    amber_cuda_ctx *c = new amber_cuda_ctx();
+    c->device = o.device;
+    c->precision = o.precision;
+    c->chunk_px = o.chunk_px;
+    c->num_sms = prop.multiProcessorCount;
+    size_t fr = 0, tot = 0;
+    cudaMemGetInfo(&fr, &tot);
+    c->budget = o.hbm_budget ? o.hbm_budget : (size_t)(0.9 * (double)fr);
+    if (o.stream) {
+        c->stream = (cudaStream_t)o.stream;
+    } else {
+        cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+        c->own_stream = true;
+    }
+    cudaEventCreate(&c->ev0);
+    cudaEventCreate(&c->ev1);
+    *out = c;
+    return AMBER_OK;
+}
+
+void amber_cuda_destroy(amber_cuda_ctx *c)
+{
+    if (!c) return;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    DevBuf *bufs[] = {&c->grid, &c->mask, &c->d_weight, &c->d_anchors, &c->y, &c->maps_d, &c->maps_i,
+                      &c->partial, &c->results, &c->ring_lohi, &c->misc, &c->mixed_scratch};
+    for (DevBuf *b : bufs) release(c, *b);
+    for (auto &kv : c->twiddles) release(c, kv.second);
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->own_stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+const char *amber_cuda_last_error(const amber_cuda_ctx *c)
+{
+    return c ? c->err.c_str() : "no context";
+}
+
+int amber_cuda_load_grid_packed(amber_cuda_ctx *c, long N1, long nc, double Du, int flag_key, const double *re_im,
+                                const double *ntig)
+{
+    if (!c) return AMBER_ERR_ARG;
+    cudaSetDevice(c->device);
+    return upload_grid(c, N1, nc, Du, flag_key, re_im, ntig);
+}
+
+int amber_cuda_load_grid(amber_cuda_ctx *c, long N1, long nc, double Du, int flag_key, const double *const *GVre,
+                         const double *const *GVim, const double *const *NTiG)
+{
+    if (!c) return AMBER_ERR_ARG;
+    if (!GVre || !GVim || !NTiG || N1 <= 0 || nc <= 0) return fail(c, AMBER_ERR_ARG, "bad grid arguments");
+    const long ncell = N1 * (N1 / 2 + 1);
+    std::vector<double> ri((size_t)ncell * nc * 2), nt((size_t)ncell * nc);
+    for (long i = 0; i < ncell; ++i) {
+        if (!GVre[i] || !GVim[i] || !NTiG[i]) return fail(c, AMBER_ERR_ARG, "NULL cell pointer at %ld", i);
+        for (long ch = 0; ch < nc; ++ch) {
+            ri[(i * nc + ch) * 2] = GVre[i][ch];
+            ri[(i * nc + ch) * 2 + 1] = GVim[i][ch];
+            nt[i * nc + ch] = NTiG[i][ch];
+        }
+    }
+    cudaSetDevice(c->device);
+    return upload_grid(c, N1, nc, Du, flag_key, ri.data(), nt.data());
+}
+
+int amber_cuda_set_rings(amber_cuda_ctx *c, int Nr, const double *ULow, const double *UHigh)
+{
+    if (!c) return AMBER_ERR_ARG;
+    if (Nr <= 0 || Nr > 255 || !ULow || !UHigh) return fail(c, AMBER_ERR_ARG, "bad ring count %d", Nr);
+    for (int r = 0; r < Nr; ++r)
+        if (!(UHigh[r] > ULow[r]) || !(ULow[r] >= 0))
+            return fail(c, AMBER_ERR_ARG, "ring %d has edges [%g, %g)", r, ULow[r], UHigh[r]);
+    c->Nr = Nr;
+    c->ulow.assign(ULow, ULow + Nr);
+    c->uhigh.assign(UHigh, UHigh + Nr);
+    c->uavg.resize(Nr);
+    for (int i = 0; i < Nr; ++i)  // amber_funcs.c:2065
+        c->uavg[i] =
+            (2. / 3.) * (pow(UHigh[i], 3.) - pow(ULow[i], 3.)) / (pow(UHigh[i], 2.) - pow(ULow[i], 2.));
+    return AMBER_OK;
+}
+
+int amber_cuda_get_uavg(const amber_cuda_ctx *c, double *Uavg)
+{
+    if (!c || !Uavg || c->Nr <= 0) return AMBER_ERR_ARG;
+    memcpy(Uavg, c->uavg.data(), sizeof(double) * c->Nr);
+    return AMBER_OK;
+}
+
+int amber_cuda_set_channels(amber_cuda_ctx *c, int nc10, int uf_nc, const int *uf_chans)
+{
+    if (!c) return AMBER_ERR_ARG;
+    if (c->nc <= 0) return fail(c, AMBER_ERR_STATE, "load the grid before the channels");
+    if (nc10 < 0 || nc10 >= c->nc) return fail(c, AMBER_ERR_ARG, "nc10=%d outside [0, nc)", nc10);
+    if (uf_nc < 0 || (uf_nc > 0 && !uf_chans)) return fail(c, AMBER_ERR_ARG, "bad uf_chans");
+    std::vector<int> w(c->nc, uf_nc > 0 ? 0 : 1);
+    for (int i = 0; i < uf_nc; ++i) {
+        if (uf_chans[i] < 0 || uf_chans[i] >= c->nc)
+            return fail(c, AMBER_ERR_ARG, "uf_chans[%d]=%d outside [0, %ld)", i, uf_chans[i], c->nc);
+        w[uf_chans[i]] += 1;
+    }
+    const int nclen = 2 * nc10 + 1;
+    // numdnu[Δ2][Δ3] = Σ_p1 w[p1]·w[p1+Δ2]·w[p1+Δ3]: the number of rows of the
+    // reference's vcp table with that lag (amber_funcs.c:2207-2310), exactly.
+    std::vector<int64_t> cnt((size_t)nclen * nclen, 0);
+    std::vector<int> anchors;
+    for (int p1 = 0; p1 < c->nc; ++p1) {
+        if (!w[p1]) continue;
+        anchors.push_back(p1);
+        for (int d2 = -nc10; d2 <= nc10; ++d2) {
+            int p2 = p1 + d2;
+            if (p2 < 0 || p2 >= c->nc || !w[p2]) continue;
+            int64_t w12 = (int64_t)w[p1] * w[p2];
+            int64_t *row = cnt.data() + (size_t)(d2 + nc10) * nclen;
+            for (int d3 = -nc10; d3 <= nc10; ++d3) {
+                int p3 = p1 + d3;
+                if (p3 < 0 || p3 >= c->nc || !w[p3]) continue;
+                row[d3 + nc10] += w12 * w[p3];
+            }
+        }
+    }
+    int rc;
+    if ((rc = ensure(c, c->d_weight, sizeof(int) * c->nc, "channel weights"))) return rc;
+    if ((rc = ensure(c, c->d_anchors, sizeof(int) * std::max<size_t>(1, anchors.size()), "anchors"))) return rc;
+    cudaSetDevice(c->device);
+    if ((rc = cuda_check(c, cudaMemcpy(c->d_weight.p, w.data(), sizeof(int) * c->nc, cudaMemcpyHostToDevice),
+                         "weights")))
+        return rc;
+    if (!anchors.empty() &&
+        (rc = cuda_check(c, cudaMemcpy(c->d_anchors.p, anchors.data(), sizeof(int) * anchors.size(),
+                                       cudaMemcpyHostToDevice),
+                         "anchors")))
+        return rc;
+    c->nc10 = nc10;
+    c->uf.assign(uf_chans, uf_chans + uf_nc);
+    c->weight = w;
+    c->anchors = anchors;
+    c->counts = cnt;
+    c->total_vcp = 0;
+    for (int64_t v : cnt) c->total_vcp += v;
+    return AMBER_OK;
+}
+
+long amber_cuda_ng1(const amber_cuda_ctx *c, int r1)
+{
+    if (!c || r1 < 0 || r1 >= c->Nr || !(c->Du > 0)) return -1;
+    return ng1_of(c->uhigh[r1], c->Du);
+}
+
+int amber_cuda_calcr(amber_cuda_ctx *c, int max_tri, int *rcount, double *rdata)
+{
+    if (!c || !rcount || (max_tri > 0 && !rdata)) return AMBER_ERR_ARG;
+    int rc = check_ready(c, false);
+    if (rc) return rc;
+    const int plane = 5;  // calCR reads the channel-5 mask, amber_funcs.c:427
+    if (c->nc <= plane) return fail(c, AMBER_ERR_ARG, "calCR reads channel %d but nc=%ld", plane, c->nc);
+    cudaSetDevice(c->device);
+    const long n1 = c->N1, k = n1 * n1;
+    if ((rc = ensure(c, c->maps_i, sizeof(double) * (size_t)c->Nr * k, "calCR mask maps"))) return rc;
+    MapJob job{};
+    job.src = c->mask.p;
+    job.src_complex = false;
+    job.n1 = n1;
+    job.nc = c->nc;
+    job.chan_base = plane;
+    job.nch = 1;
+    job.ng = n1;
+    job.kp = k;
+    job.nslots = c->Nr;
+    job.lo = c->ulow;
+    job.hi = c->uhigh;
+    job.out_f64 = (double *)c->maps_i.p;
+    if ((rc = build_maps(c, job))) return rc;
+    std::vector<int> tri;
+    for (int r1 = 0; r1 < c->Nr; ++r1)
+        for (int r2 = 0; r2 <= r1; ++r2)
+            for (int r3 = 0; r3 <= r2; ++r3)
+                if (closed(c->uavg, r1, r2, r3)) {
+                    tri.push_back(r1);
+                    tri.push_back(r2);
+                    tri.push_back(r3);
+                }
+    const int n = (int)tri.size() / 3;
+    if ((rc = ensure(c, c->results, sizeof(double) * std::max(1, n), "calCR sums"))) return rc;
+    const double *II = (const double *)c->maps_i.p;
+    for (int t = 0; t < n; ++t)
+        if ((rc = triple_sum(c, II + (long)tri[3 * t] * k, II + (long)tri[3 * t + 1] * k,
+                             II + (long)tri[3 * t + 2] * k, k, (double *)c->results.p + t)))
+            return rc;
+    std::vector<double> num(std::max(1, n));
+    if ((rc = cuda_check(c, cudaMemcpyAsync(num.data(), c->results.p, sizeof(double) * n, cudaMemcpyDeviceToHost,
+                                            c->stream),
+                         "calCR download")))
+        return rc;
+    if ((rc = cuda_check(c, cudaStreamSynchronize(c->stream), "calCR"))) return rc;
+    *rcount = n;
+    for (int t = 0; t < n && t < max_tri; ++t) {
+        rdata[4 * t] = tri[3 * t];
+        rdata[4 * t + 1] = tri[3 * t + 1];
+        rdata[4 * t + 2] = tri[3 * t + 2];
+        rdata[4 * t + 3] = num[t];
+    }
+    return AMBER_OK;
+}
+
+int amber_cuda_triangles_run(amber_cuda_ctx *c, int ntri, const int *tri, int want_v2)
+{
+    if (!c || ntri < 0 || (ntri > 0 && !tri)) return AMBER_ERR_ARG;
+    int rc = check_ready(c, true);
+    if (rc) return rc;
+    for (int t = 0; t < ntri; ++t) {
+        int r1 = tri[3 * t], r2 = tri[3 * t + 1], r3 = tri[3 * t + 2];
+        if (r1 < 0 || r1 >= c->Nr || r2 < 0 || r2 >= c->Nr || r3 < 0 || r3 >= c->Nr)
+            return fail(c, AMBER_ERR_ARG, "triangle %d has a ring outside [0, %d)", t, c->Nr);
+    }
+    cudaSetDevice(c->device);
+    const int nclen = 2 * c->nc10 + 1;
+    const long ncsize = (long)nclen * nclen;
+    if ((rc = ensure(c, c->results, sizeof(double) * 2 * ncsize * std::max(1, ntri), "results"))) return rc;
+    double *res = (double *)c->results.p;
+
+    // group by r1: every ring of a group lives on the group's Ng1 grid
+    std::vector<Group> groups;
+    for (int t = 0; t < ntri; ++t) {
+        int r1 = tri[3 * t];
+        long ng = ng1_of(c->uhigh[r1], c->Du);
+        auto it = std::find_if(groups.begin(), groups.end(), [&](const Group &g) { return g.r1 == r1; });
+        if (it == groups.end()) {
+            groups.push_back(Group{r1, ng, {}});
+            it = groups.end() - 1;
+        }
+        it->tris.push_back(t);
+    }
+    const bool mixed = c->precision == AMBER_PREC_MIXED;
+    const size_t vbytes = mixed ? 4 : 8;  // per map value: hi+lo bf16, or FP64
+    c->last_products = 0;
+    cudaEventRecord(c->ev0, c->stream);
+    for (const Group &g : groups) {
+        const long k = g.ng * g.ng, kp = (k + 63) / 64 * 64;
+        const size_t per_slot = vbytes * (size_t)c->nc * kp;
+        // Process the group's triangles in batches whose ring union fits the budget.
+        size_t spare = c->budget > c->held ? c->budget - c->held : 0;
+        spare += c->maps_d.bytes + c->maps_i.bytes;
+        size_t reserve = (size_t)64 << 20;
+        long cap_slots = (long)((spare > reserve ? spare - reserve : 0) / (per_slot * (want_v2 ? 2 : 1) + 1));
+        if (cap_slots < 3) return fail(c, AMBER_ERR_OOM, "maps of one triangle (Ng1=%ld) exceed the budget", g.ng);
+        size_t ti = 0;
+        while (ti < g.tris.size()) {
+            std::vector<int> batch;
+            std::set<int> rings;
+            while (ti < g.tris.size()) {
+                int t = g.tris[ti];
+                std::set<int> u = rings;
+                u.insert(tri[3 * t]);
+                u.insert(tri[3 * t + 1]);
+                u.insert(tri[3 * t + 2]);
+                if ((long)u.size() > cap_slots) break;
+                rings = u;
+                batch.push_back(t);
+                ++ti;
+            }
+            MapSet ms;
+            ms.ng = g.ng;
+            ms.k = k;
+            ms.kp = kp;
+            for (int i = 0; i < 256; ++i) ms.slot_of_ring[i] = -1;
+            for (int r : rings) {
+                ms.slot_of_ring[r] = (int)ms.ring_of_slot.size();
+                ms.ring_of_slot.push_back(r);
+            }
+            ms.nslots = (int)ms.ring_of_slot.size();
+            if ((rc = ensure(c, c->maps_d, per_slot * ms.nslots, "ring maps"))) return rc;
+            if (want_v2 && (rc = ensure(c, c->maps_i, per_slot * ms.nslots, "ring mask maps"))) return rc;
+            for (int pass = 0; pass < (want_v2 ? 2 : 1); ++pass) {
+                MapJob job{};
+                job.src = pass == 0 ? c->grid.p : c->mask.p;
+                job.src_complex = pass == 0;
+                job.n1 = c->N1;
+                job.nc = c->nc;
+                job.chan_base = 0;
+                job.nch = c->nc;
+                job.ng = g.ng;
+                job.kp = kp;
+                job.nslots = ms.nslots;
+                for (int r : ms.ring_of_slot) {
+                    job.lo.push_back(c->ulow[r]);
+                    job.hi.push_back(c->uhigh[r]);
+                }
+                void *base = pass == 0 ? c->maps_d.p : c->maps_i.p;
+                if (mixed) {
+                    job.out_hi = (uint16_t *)base;
+                    job.out_lo = (uint16_t *)base + (size_t)ms.nslots * c->nc * kp;
+                } else {
+                    job.out_f64 = (double *)base;
+                }
+                if ((rc = build_maps(c, job))) return rc;
+            }
+            for (int t : batch) {
+                int s1 = ms.slot_of_ring[tri[3 * t]], s2 = ms.slot_of_ring[tri[3 * t + 1]],
+                    s3 = ms.slot_of_ring[tri[3 * t + 2]];
+                for (int pass = 0; pass < (want_v2 ? 2 : 1); ++pass) {
+                    void *base = pass == 0 ? c->maps_d.p : c->maps_i.p;
+                    double *lag = res + ((size_t)t * 2 + pass) * ncsize;
+                    if (mixed) {
+                        const uint16_t *hi = (const uint16_t *)base;
+                        const uint16_t *lo = hi + (size_t)ms.nslots * c->nc * kp;
+                        const size_t ss = (size_t)c->nc * kp;
+                        rc = contract_mixed(c, hi + s1 * ss, lo + s1 * ss, hi + s2 * ss, lo + s2 * ss, hi + s3 * ss,
+                                            lo + s3 * ss, k, kp, lag);
+                    } else {
+                        const double *m = (const double *)base;
+                        const size_t ss = (size_t)c->nc * kp;
+                        rc = contract_fp64(c, m + s1 * ss, m + s2 * ss, m + s3 * ss, k, kp, lag);
+                    }
+                    if (rc) return rc;
+                }
+                c->last_products += (double)c->total_vcp * (double)k * (want_v2 ? 2.0 : 1.0);
+            }
+        }
+    }
+    cudaEventRecord(c->ev1, c->stream);
+    if ((rc = cuda_check(c, cudaEventSynchronize(c->ev1), "triangle run"))) return rc;
+    if ((rc = cuda_check(c, cudaGetLastError(), "triangle run"))) return rc;
+    cudaEventElapsedTime(&c->last_ms, c->ev0, c->ev1);
+    c->last_ntri = ntri;
+    c->last_v2 = want_v2;
+    return AMBER_OK;
+}
+
+int amber_cuda_triangles_fetch(amber_cuda_ctx *c, double *bldnu, int64_t *numdnu, double *numtri)
+{
+    if (!c) return AMBER_ERR_ARG;
+    const int nclen = 2 * c->nc10 + 1;
+    const long ncsize = (long)nclen * nclen;
+    const int n = c->last_ntri;
+    int rc;
+    cudaSetDevice(c->device);
+    for (int t = 0; t < n; ++t) {
+        const double *src = (const double *)c->results.p + (size_t)t * 2 * ncsize;
+        if (bldnu &&
+            (rc = cuda_check(c, cudaMemcpyAsync(bldnu + (size_t)t * ncsize, src, sizeof(double) * ncsize,
+                                                cudaMemcpyDeviceToHost, c->stream),
+                             "fetch bldnu")))
+            return rc;
+        if (numtri && c->last_v2 &&
+            (rc = cuda_check(c, cudaMemcpyAsync(numtri + (size_t)t * ncsize, src + ncsize, sizeof(double) * ncsize,
+                                                cudaMemcpyDeviceToHost, c->stream),
+                             "fetch numtri")))
+            return rc;
+        if (numdnu) memcpy(numdnu + (size_t)t * ncsize, c->counts.data(), sizeof(int64_t) * ncsize);
+    }
+    return cuda_check(c, cudaStreamSynchronize(c->stream), "fetch");
+}
+
+int amber_cuda_triangles(amber_cuda_ctx *c, int ntri, const int *tri, int want_v2, double *bldnu, int64_t *numdnu,
+                         double *numtri)
+{
+    int rc = amber_cuda_triangles_run(c, ntri, tri, want_v2);
+    if (rc) return rc;
+    return amber_cuda_triangles_fetch(c, bldnu, numdnu, numtri);
+}
+
+int amber_cuda_last_run_stats(const amber_cuda_ctx *c, double *products, double *device_ms)
+{
+    if (!c) return AMBER_ERR_ARG;
+    if (products) *products = c->last_products;
+    if (device_ms) *device_ms = c->last_ms;
+    return AMBER_OK;
+}
+
+int amber_cuda_triangle_v1(amber_cuda_ctx *c, int r1, int r2, int r3, double rdata_num, float *bldnu,
+                           int32_t *numdnu, double *Ntri, double *Num)
+{
+    if (!c || !bldnu || !numdnu) return AMBER_ERR_ARG;
+    int tri[3] = {r1, r2, r3};
+    int rc = amber_cuda_triangles_run(c, 1, tri, 0);
+    if (rc) return rc;
+    const int nclen = 2 * c->nc10 + 1;
+    const long ncsize = (long)nclen * nclen;
+    std::vector<double> bl(ncsize);
+    if ((rc = amber_cuda_triangles_fetch(c, bl.data(), nullptr, nullptr))) return rc;
+    for (long i = 0; i < ncsize; ++i) {
+        if (c->counts[i] > INT32_MAX)
+            return fail(c, AMBER_ERR_OVERFLOW, "lag cell %ld holds %lld triplets, beyond int32", i,
+                        (long long)c->counts[i]);
+        bldnu[i] = (float)bl[i];
+        numdnu[i] = (int32_t)c->counts[i];
+    }
+    // per-triangle scalars, amber.c:193-202,287
+    long ng = ng1_of(c->uhigh[r1], c->Du);
+    double gfact = (1. * ng) / (1. * c->N1);
+    double num = gfact * gfact * rdata_num;
+    double inv = 1.0 / (ng * ng * 1.);
+    if (Num) *Num = num;
+    if (Ntri) *Ntri = num * inv;
+    return AMBER_OK;
+}
+
+int amber_cuda_triangle_v2(amber_cuda_ctx *c, int r1, int r2, int r3, float *bldnu, float *numdnu,
+                           double *inv_Ng1_Ng2)
+{
+    if (!c || !bldnu || !numdnu) return AMBER_ERR_ARG;
+    int tri[3] = {r1, r2, r3};
+    int rc = amber_cuda_triangles_run(c, 1, tri, 1);
+    if (rc) return rc;
+    const int nclen = 2 * c->nc10 + 1;
+    const long ncsize = (long)nclen * nclen;
+    std::vector<double> bl(ncsize), nt(ncsize);
+    if ((rc = amber_cuda_triangles_fetch(c, bl.data(), nullptr, nt.data()))) return rc;
+    for (long i = 0; i < ncsize; ++i) {
+        bldnu[i] = (float)bl[i];
+        numdnu[i] = (float)nt[i];
+    }
+    long ng = ng1_of(c->uhigh[r1], c->Du);
+    if (inv_Ng1_Ng2) *inv_Ng1_Ng2 = 1.0 / (ng * ng * 1.);
+    return AMBER_OK;
+}
+
+}  // extern "C"

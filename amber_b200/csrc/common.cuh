@@ -1,0 +1,124 @@
+// Internal declarations shared by the libamber_cuda translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/amber_cuda.h"
+
+namespace amber {
+
+// A device allocation owned by the context; grows on demand, never shrinks
+// until the context is destroyed.
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+};
+
+// One set of ring maps on a common Ng1 × Ng1 grid: maps[slot][ch][x], row
+// stride kp elements (kp = Ng1² rounded up to 64).
+struct MapSet {
+    long ng = 0;
+    long k = 0;
+    long kp = 0;
+    int nslots = 0;
+    std::vector<int> ring_of_slot;
+    int slot_of_ring[256];
+};
+
+}  // namespace amber
+
+struct amber_cuda_ctx {
+    int device = 0;
+    int precision = AMBER_PREC_FP64;
+    size_t budget = 0;
+    size_t held = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int chunk_px = 0;
+    int num_sms = 148;
+    std::string err;
+
+    // grid (normalised on the device)
+    long N1 = 0, nc = 0;
+    double Du = 0;
+    int flag_key = -1;
+    amber::DevBuf grid;  // double2 [cell][nc]
+    amber::DevBuf mask;  // double  [cell][nc] (0/1)
+
+    // rings
+    int Nr = 0;
+    std::vector<double> ulow, uhigh, uavg;
+
+    // channels
+    int nc10 = -1;
+    std::vector<int> uf;       // as given
+    std::vector<int> weight;   // multiplicity per channel (length nc)
+    std::vector<int> anchors;  // channels with weight > 0, ascending
+    std::vector<int64_t> counts;  // closed-form numdnu, nclen²
+    int64_t total_vcp = 0;
+    amber::DevBuf d_weight, d_anchors;
+
+    // twiddle tables e^{2πik/N}, per N
+    std::map<long, amber::DevBuf> twiddles;
+
+    // working buffers
+    amber::DevBuf y;        // pass-1 intermediate
+    amber::DevBuf maps_d;   // D maps (FP64 path: double; mixed path: split planes)
+    amber::DevBuf maps_i;   // I maps (v2)
+    amber::DevBuf partial;  // per-anchor/k-split partial lag tiles
+    amber::DevBuf results;  // per-triangle FP64 lag arrays [ntri][2][nclen²]
+    amber::DevBuf ring_lohi;
+    amber::DevBuf misc;
+    amber::DevBuf mixed_scratch;
+
+    // last run
+    int last_ntri = 0;
+    int last_v2 = 0;
+    double last_products = 0;
+    float last_ms = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+namespace amber {
+
+int fail(amber_cuda_ctx *c, int code, const char *fmt, ...);
+int cuda_check(amber_cuda_ctx *c, cudaError_t e, const char *what);
+int ensure(amber_cuda_ctx *c, DevBuf &b, size_t bytes, const char *what);
+int twiddle_table(amber_cuda_ctx *c, long n, const double2 **out);
+
+// Map builder: ring-mask + unnormalised c2r of every channel of the given
+// rings onto an ng × ng grid.  src_complex: double2 grid; else real mask.
+// Writes FP64 maps (out_f64) or split-BF16 hi/lo planes (out_hi/out_lo)
+// with row stride kp.  chan_base/nch select source channels.
+struct MapJob {
+    const void *src;
+    bool src_complex;
+    long n1, nc;         // source grid side and channel count
+    long chan_base, nch; // source channel window
+    long ng, kp;         // output side and row stride
+    int nslots;
+    const double *lohi;  // device: lo[s], hi[s] interleaved
+    std::vector<double> lo, hi;  // host copies
+    double *out_f64;
+    uint16_t *out_hi, *out_lo;  // bf16 planes
+    float *out_f32;
+};
+int build_maps(amber_cuda_ctx *c, const MapJob &job);
+
+// FP64 contraction of one triangle into a lag array (device).
+int contract_fp64(amber_cuda_ctx *c, const double *m1, const double *m2, const double *m3, long k, long kp,
+                  double *lag_out);
+// Mixed-precision contraction (split-BF16×3, tcgen05/TMEM).
+int contract_mixed(amber_cuda_ctx *c, const uint16_t *h1, const uint16_t *l1, const uint16_t *h2,
+                   const uint16_t *l2, const uint16_t *h3, const uint16_t *l3, long k, long kp, double *lag_out);
+// lag[d] = Σ_u partial[u][d] (compensated, fixed order).
+int lag_reduce(amber_cuda_ctx *c, const double *partial, long nunits, long ncsize, double *lag);
+// Σ_x a·b·c over n points (FP64, deterministic) into out[0].
+int triple_sum(amber_cuda_ctx *c, const double *a, const double *b, const double *cc, long n, double *out);
+
+}  // namespace amber

@@ -1,0 +1,222 @@
+// Plain FP64 triple-product lag accumulation (the reference loop of
+// 4_fbe/amber.c:247-279 restated for the GPU in FP64), the deterministic lag
+// reduction shared with the mixed-precision path, and the FP64 triple sum
+// that gives calCR's normaliser (amber_funcs.c:451-457).
+//
+// For a triangle (r1, r2, r3) with maps D1, D2, D3 [channel][pixel] the
+// reference sums, over every admissible channel triplet (p1, p2, p3) with
+// |p2−p1|, |p3−p1| ≤ nc10, Σ_x D1[p1,x]·D2[p2,x]·D3[p3,x] into the lag cell
+// (p2−p1+nc10, p3−p1+nc10).  For one anchor p1 that is the matrix
+// T_p1 = (D2 ∘ D1[p1])·D3ᵀ restricted to the p1 window.  Each CTA here owns a
+// 64 × 64 tile of one anchor's window over one pixel range: it stages
+// D1[p1]·D2 and D3 for 16 pixels at a time in shared memory and accumulates a
+// 4 × 4 register block per thread in FP64.  Channel multiplicities
+// (flagging) weight the tile when it is written.  Tiles go to a partial
+// buffer [anchor][k-split][lag2][lag3]; lag_reduce sums that buffer per lag
+// cell in a fixed order with a compensated (TwoSum) accumulator, so results
+// are deterministic and independent of the launch shape.
+#include <algorithm>
+
+#include "common.cuh"
+
+namespace amber {
+
+namespace {
+
+constexpr int TT = 64;  // tile edge in channels
+constexpr int KB = 16;  // pixels per shared-memory stage
+
+__global__ void __launch_bounds__(256) contract64_kernel(const double *__restrict__ m1, const double *__restrict__ m2,
+                                                          const double *__restrict__ m3, long k, long kp,
+                                                          const int *__restrict__ anchors,
+                                                          const int *__restrict__ weight, int nc, int nc10, int tiles,
+                                                          long kchunk, double *__restrict__ partial)
+{
+    // rows padded by 2 doubles: the transposed stores hit 8 distinct bank pairs
+    __shared__ __align__(16) double As[2][KB][TT + 2];
+    __shared__ __align__(16) double Bs[2][KB][TT + 2];
+    const int tid = threadIdx.x;
+    const int a = blockIdx.y, ks = blockIdx.z, KS = gridDim.z;
+    const int t2 = blockIdx.x / tiles, t3 = blockIdx.x % tiles;
+    const int p1 = anchors[a];
+    const int nclen = 2 * nc10 + 1;
+    const int d2b = TT * t2, d3b = TT * t3;
+    const int tx = tid & 15, ty = tid >> 4;
+    double *out = partial + ((size_t)a * KS + ks) * nclen * nclen;
+
+    // rows (p2) and columns (p3) this tile covers; -1 marks an empty row/col
+    __shared__ int prow[TT], pcol[TT];
+    __shared__ int any_row, any_col;
+    if (tid == 0) { any_row = 0; any_col = 0; }
+    __syncthreads();
+    if (tid < TT) {
+        int d = d2b + tid, p = p1 - nc10 + d;
+        bool ok = d < nclen && p >= 0 && p < nc && weight[p] > 0;
+        prow[tid] = ok ? p : -1;
+        if (ok) atomicOr(&any_row, 1);
+    } else if (tid < 2 * TT) {
+        int d = d3b + tid - TT, p = p1 - nc10 + d;
+        bool ok = d < nclen && p >= 0 && p < nc && weight[p] > 0;
+        pcol[tid - TT] = ok ? p : -1;
+        if (ok) atomicOr(&any_col, 1);
+    }
+    __syncthreads();
+
+    double acc[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+
+    const long x0 = (long)ks * kchunk, x1 = min(k, x0 + kchunk);
+    if (any_row && any_col && x0 < x1) {
+        const double *c1 = m1 + (long)p1 * kp;
+        // each thread loads 4 elements of A and 4 of B per stage
+        auto load = [&](int buf, long xs) {
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                int e = tid + i * 256;
+                int r = e / KB, xx = e % KB;
+                long x = xs + xx;
+                double va = 0.0, vb = 0.0;
+                if (x < x1) {
+                    int pr = prow[r], pc = pcol[r];
+                    double s1 = c1[x];
+                    if (pr >= 0) va = s1 * m2[(long)pr * kp + x];
+                    if (pc >= 0) vb = m3[(long)pc * kp + x];
+                }
+                As[buf][xx][r] = va;
+                Bs[buf][xx][r] = vb;
+            }
+        };
+        int buf = 0;
+        load(0, x0);
+        __syncthreads();
+        for (long xs = x0; xs < x1; xs += KB) {
+            if (xs + KB < x1) load(buf ^ 1, xs + KB);
+#pragma unroll
+            for (int xx = 0; xx < KB; ++xx) {
+                double2 a01 = *reinterpret_cast<const double2 *>(&As[buf][xx][ty * 4]);
+                double2 a23 = *reinterpret_cast<const double2 *>(&As[buf][xx][ty * 4 + 2]);
+                double2 b01 = *reinterpret_cast<const double2 *>(&Bs[buf][xx][tx * 4]);
+                double2 b23 = *reinterpret_cast<const double2 *>(&Bs[buf][xx][tx * 4 + 2]);
+                double av[4] = {a01.x, a01.y, a23.x, a23.y};
+                double bv[4] = {b01.x, b01.y, b23.x, b23.y};
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
+            }
+            __syncthreads();
+            buf ^= 1;
+        }
+    }
+    const double w1 = (double)weight[p1];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        int r = ty * 4 + i, d2 = d2b + r;
+        if (d2 >= nclen) continue;
+        int pr = prow[r];
+        double wr = pr >= 0 ? w1 * (double)weight[pr] : 0.0;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            int cc = tx * 4 + j, d3 = d3b + cc;
+            if (d3 >= nclen) continue;
+            int pc = pcol[cc];
+            double wc = pc >= 0 ? (double)weight[pc] : 0.0;
+            out[(long)d2 * nclen + d3] = acc[i][j] * wr * wc;
+        }
+    }
+}
+
+// lag[d] = Σ_{u < nunits} partial[u][d], TwoSum-compensated, fixed order.
+__global__ void lag_reduce_kernel(const double *__restrict__ partial, long nunits, long ncsize,
+                                  double *__restrict__ lag)
+{
+    long d = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (d >= ncsize) return;
+    double s = 0.0, comp = 0.0;
+    for (long u = 0; u < nunits; ++u) {
+        double v = partial[u * ncsize + d];
+        double t = s + v;
+        double bp = t - s;
+        comp += (s - (t - bp)) + (v - bp);
+        s = t;
+    }
+    lag[d] = s + comp;
+}
+
+__global__ void triple_sum_partial(const double *__restrict__ a, const double *__restrict__ b,
+                                   const double *__restrict__ c, long n, double *__restrict__ part)
+{
+    __shared__ double red[256];
+    double s = 0.0;
+    for (long i = (long)blockIdx.x * 256 + threadIdx.x; i < n; i += (long)gridDim.x * 256) s += a[i] * b[i] * c[i];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = red[0];
+}
+
+__global__ void sum_fixed(const double *__restrict__ part, int n, double *__restrict__ out)
+{
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        double s = 0.0, comp = 0.0;
+        for (int i = 0; i < n; ++i) {
+            double t = s + part[i];
+            double bp = t - s;
+            comp += (s - (t - bp)) + (part[i] - bp);
+            s = t;
+        }
+        out[0] = s + comp;
+    }
+}
+
+}  // namespace
+
+int lag_reduce(amber_cuda_ctx *c, const double *partial, long nunits, long ncsize, double *lag)
+{
+    lag_reduce_kernel<<<(unsigned)((ncsize + 255) / 256), 256, 0, c->stream>>>(partial, nunits, ncsize, lag);
+    return cuda_check(c, cudaGetLastError(), "lag_reduce_kernel launch");
+}
+
+int contract_fp64(amber_cuda_ctx *c, const double *m1, const double *m2, const double *m3, long k, long kp,
+                  double *lag_out)
+{
+    const int nc10 = c->nc10;
+    const int nclen = 2 * nc10 + 1;
+    const long ncsize = (long)nclen * nclen;
+    const int nA = (int)c->anchors.size();
+    if (nA == 0) return cuda_check(c, cudaMemsetAsync(lag_out, 0, sizeof(double) * ncsize, c->stream), "zero lag");
+    const int tiles = (nclen + TT - 1) / TT;
+    long blocks = (long)tiles * tiles * nA;
+    long want = 4L * c->num_sms;
+    int KS = (int)std::max<long>(1, std::min<long>((want + blocks - 1) / blocks, (k + 1023) / 1024));
+    long kchunk = ((k + KS - 1) / KS + KB - 1) / KB * KB;
+    KS = (int)((k + kchunk - 1) / kchunk);
+    if (KS < 1) KS = 1;
+    size_t pbytes = sizeof(double) * (size_t)nA * KS * ncsize;
+    int rc = ensure(c, c->partial, pbytes, "partial lag tiles");
+    if (rc) return rc;
+    dim3 grid((unsigned)(tiles * tiles), (unsigned)nA, (unsigned)KS);
+    contract64_kernel<<<grid, 256, 0, c->stream>>>(m1, m2, m3, k, kp, (const int *)c->d_anchors.p,
+                                                   (const int *)c->d_weight.p, (int)c->nc, nc10, tiles, kchunk,
+                                                   (double *)c->partial.p);
+    if ((rc = cuda_check(c, cudaGetLastError(), "contract64_kernel launch"))) return rc;
+    return lag_reduce(c, (const double *)c->partial.p, (long)nA * KS, ncsize, lag_out);
+}
+
+int triple_sum(amber_cuda_ctx *c, const double *a, const double *b, const double *cc, long n, double *out)
+{
+    const int nb = 256;
+    int rc = ensure(c, c->misc, sizeof(double) * nb, "triple-sum partials");
+    if (rc) return rc;
+    triple_sum_partial<<<nb, 256, 0, c->stream>>>(a, b, cc, n, (double *)c->misc.p);
+    sum_fixed<<<1, 32, 0, c->stream>>>((const double *)c->misc.p, nb, out);
+    return cuda_check(c, cudaGetLastError(), "triple_sum launch");
+}
+
+}  // namespace amber

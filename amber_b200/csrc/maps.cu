@@ -1,0 +1,354 @@
+// Ring filter + unnormalised 2D c2r, fused and batched over (ring × channel).
+//
+// Replaces Dfg/Ifg + fill_s2d_float/fill_s2I (4_fbe/amber_funcs.c:573-621,
+// 967-1010, 1109-1131) and the mask transform inside calCR (389-437).  For a
+// ring [lo, hi) the reference scatters grid cell (ia mod N1, j) into bin
+// (ia mod Ng1, j) of a zeroed Ng1 × (Ng1/2+1) half-plane for ia ∈ (−Ng1/2,
+// Ng1/2], j < Ng1/3, lo ≤ √(ia²+j²) < hi, √ > 0, then runs
+// fftw_plan_dft_c2r_2d.  Only |ia|, j < hi are ever non-zero, so instead of a
+// full FFT of a mostly-empty plane we evaluate the transform directly on the
+// non-zero support ("pruned DFT"), which is exact for any Ng1 — the map sides
+// here have large prime factors (740 = 4·5·37, 1460 = 4·5·73):
+//
+//   pass 1 (axis 0, per column j < J):  Y[n0][j] = Σ_ia X[ia][j] · e^{+2πi·ia·n0/Ng1}
+//   pass 2 (axis 1, c2r):               D[n0][n1] = Re Y[n0][0] + 2 Σ_{j≥1} Re(Y[n0][j] · e^{+2πi·j·n1/Ng1})
+//
+// The c2r convention — complex DFT along axis 0, then a 1D c2r along axis 1
+// that ignores Im of bin 0 — is what a rank-2 c2r does with the non-Hermitian
+// j = 0 column the ring scatter produces; the Nyquist bin j = Ng1/2 is never
+// filled because j < Ng1/3.
+//
+// Both passes stage one column / one row of the spectrum for C channels in
+// shared memory together with the twiddle table e^{2πik/Ng1}; lanes of a warp
+// walk channels (coalesced loads of the channel-innermost grid and of Y) and
+// share one twiddle per step (a shared-memory broadcast).  Twiddle indices
+// advance incrementally (k += n mod Ng1), so the inner loop is FP64 FMA work.
+// All arithmetic is FP64.
+#include <cuda_bf16.h>
+#include <math.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "common.cuh"
+
+namespace amber {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+// Rows of column j that fall inside ring [lo, hi) for an ng-point output grid.
+__device__ __forceinline__ bool in_ring(long ia, long j, double lo, double hi)
+{
+    double uu = sqrt(1.0 * (double)(ia * ia + j * j));
+    return uu >= lo && uu < hi && uu > 0.0;
+}
+
+template <int C>
+__global__ void __launch_bounds__(kThreads) ring_cols_kernel(const void *__restrict__ src, int src_complex, long n1,
+                                                              long nc, long chan_base, long nch, long ng,
+                                                              const double *__restrict__ lohi,
+                                                              const int *__restrict__ jcols, int jmax,
+                                                              const double2 *__restrict__ tw_g,
+                                                              double2 *__restrict__ Y, int rowcap)
+{
+    extern __shared__ double2 smem[];
+    double2 *tw = smem;                        // ng
+    double2 *xs = tw + ng;                     // rowcap × C
+    int *ias = reinterpret_cast<int *>(xs + (size_t)rowcap * C);  // rowcap
+    __shared__ int warp_cnt[kThreads / 32];
+    __shared__ int nrows_s;
+
+    const int j = blockIdx.x, s = blockIdx.y;
+    const long q0 = (long)blockIdx.z * C;
+    if (j >= jcols[s]) return;
+    const double lo = lohi[2 * s], hi = lohi[2 * s + 1];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const long h1 = n1 / 2 + 1;
+
+    for (long i = tid; i < ng; i += kThreads) tw[i] = tw_g[i];
+
+    // Ordered compaction of the ring's rows in this column.
+    const long A = (long)ceil(hi) - 1;
+    const long ia_min = max(-A, -ng / 2 + 1), ia_max = min(A, ng / 2);
+    if (tid == 0) nrows_s = 0;
+    __syncthreads();
+    for (long base = ia_min; base <= ia_max; base += kThreads) {
+        long ia = base + tid;
+        bool hit = ia <= ia_max && in_ring(ia, j, lo, hi);
+        unsigned m = __ballot_sync(0xffffffffu, hit);
+        if (lane == 0) warp_cnt[warp] = __popc(m);
+        __syncthreads();
+        int off = nrows_s;
+        for (int w = 0; w < warp; ++w) off += warp_cnt[w];
+        off += __popc(m & ((1u << lane) - 1u));
+        if (hit && off < rowcap) ias[off] = (int)ia;
+        __syncthreads();
+        if (tid == 0) {
+            int tot = 0;
+            for (int w = 0; w < kThreads / 32; ++w) tot += warp_cnt[w];
+            nrows_s += tot;
+        }
+        __syncthreads();
+    }
+    const int nrows = min(nrows_s, rowcap);
+
+    // Gather the ring's cells for C channels (channel-innermost: coalesced).
+    for (int e = tid; e < nrows * C; e += kThreads) {
+        int r = e / C, q = e % C;
+        long ia = ias[r];
+        long iN = ia < 0 ? n1 + ia : ia;
+        long cell = iN * h1 + j;
+        double2 v = make_double2(0.0, 0.0);
+        if (q0 + q < nch) {
+            long ch = chan_base + q0 + q;
+            if (src_complex)
+                v = reinterpret_cast<const double2 *>(src)[cell * nc + ch];
+            else
+                v.x = reinterpret_cast<const double *>(src)[cell * nc + ch];
+        }
+        xs[r * C + q] = v;
+    }
+    __syncthreads();
+
+    // Y[n0][j] for this thread's channel q and R rows n0 at a time.
+    constexpr int G = 32 / C;  // n0 groups per warp
+    constexpr int R = 4;
+    const int q = lane % C, g = lane / C;
+    const int gid = warp * G + g;
+    const int ngroups = (kThreads / 32) * G;
+    for (long nb = (long)gid; nb * R < ng; nb += ngroups) {
+        long n0[R];
+        double2 acc[R];
+        int idx[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            n0[r] = nb * R + r;
+            acc[r] = make_double2(0.0, 0.0);
+            idx[r] = 0;
+        }
+        long prev = LONG_MIN;
+        for (int row = 0; row < nrows; ++row) {
+            long ia = ias[row];
+            if (ia != prev + 1) {
+                long iam = ia < 0 ? ia + ng : ia;
+#pragma unroll
+                for (int r = 0; r < R; ++r) idx[r] = (int)((iam * (n0[r] < ng ? n0[r] : 0)) % ng);
+            } else {
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    int t = idx[r] + (int)(n0[r] < ng ? n0[r] : 0);
+                    idx[r] = t >= ng ? t - (int)ng : t;
+                }
+            }
+            prev = ia;
+            double2 x = xs[row * C + q];
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                double2 w = tw[idx[r]];
+                acc[r].x = fma(x.x, w.x, acc[r].x);
+                acc[r].x = fma(-x.y, w.y, acc[r].x);
+                acc[r].y = fma(x.x, w.y, acc[r].y);
+                acc[r].y = fma(x.y, w.x, acc[r].y);
+            }
+        }
+        if (q0 + q < nch) {
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+                if (n0[r] < ng) Y[(((long)s * ng + n0[r]) * jmax + j) * nch + q0 + q] = acc[r];
+        }
+    }
+}
+
+__device__ __forceinline__ uint16_t bf16_bits(float f)
+{
+    __nv_bfloat16 b = __float2bfloat16_rn(f);
+    return *reinterpret_cast<uint16_t *>(&b);
+}
+
+template <int C>
+__global__ void __launch_bounds__(kThreads) ring_rows_kernel(const double2 *__restrict__ Y, long ng, int jmax,
+                                                              const int *__restrict__ jcols, long nch,
+                                                              const double2 *__restrict__ tw_g, long kp,
+                                                              double *__restrict__ out_f64,
+                                                              uint16_t *__restrict__ out_hi,
+                                                              uint16_t *__restrict__ out_lo,
+                                                              float *__restrict__ out_f32)
+{
+    extern __shared__ double2 smem[];
+    double2 *tw = smem;       // ng
+    double2 *ys = tw + ng;    // J × C
+    const long n0 = blockIdx.x;
+    const int s = blockIdx.y;
+    const long q0 = (long)blockIdx.z * C;
+    const int J = jcols[s];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (long i = tid; i < ng; i += kThreads) tw[i] = tw_g[i];
+    for (int e = tid; e < J * C; e += kThreads) {
+        int jj = e / C, q = e % C;
+        double2 v = make_double2(0.0, 0.0);
+        if (q0 + q < nch) v = Y[(((long)s * ng + n0) * jmax + jj) * nch + q0 + q];
+        if (jj == 0) v.y = 0.0;  // c2r ignores Im of the DC bin
+        else { v.x *= 2.0; v.y *= 2.0; }
+        ys[e] = v;
+    }
+    __syncthreads();
+
+    constexpr int G = 32 / C;
+    constexpr int R = 8;
+    const int q = lane % C, g = lane / C;
+    const int gid = warp * G + g;
+    const int ngroups = (kThreads / 32) * G;
+    const long slot_row = ((long)s * nch + q0 + q) * kp + n0 * ng;
+    for (long nb = gid; nb * R < ng; nb += ngroups) {
+        double acc[R];
+        int idx[R], step[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            long n1 = nb * R + r;
+            step[r] = (int)(n1 < ng ? n1 : 0);
+            idx[r] = 0;
+            acc[r] = 0.0;
+        }
+        for (int jj = 0; jj < J; ++jj) {
+            double2 y = ys[jj * C + q];
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                double2 w = tw[idx[r]];
+                acc[r] = fma(y.x, w.x, acc[r]);
+                acc[r] = fma(-y.y, w.y, acc[r]);
+                int t = idx[r] + step[r];
+                idx[r] = t >= ng ? t - (int)ng : t;
+            }
+        }
+        if (q0 + q < nch) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                long n1 = nb * R + r;
+                if (n1 >= ng) continue;
+                long o = slot_row + n1;
+                double v = acc[r];
+                if (out_f64) out_f64[o] = v;
+                if (out_f32) out_f32[o] = (float)v;
+                if (out_hi) {
+                    // split: hi = bf16(v), lo = bf16(v − hi) (both round-to-nearest)
+                    float f = (float)v;
+                    uint16_t h = bf16_bits(f);
+                    float hf = __uint_as_float((uint32_t)h << 16);
+                    out_hi[o] = h;
+                    out_lo[o] = bf16_bits((float)(v - (double)hf));
+                }
+            }
+        }
+    }
+}
+
+// Host: exact per-slot column counts and the largest number of ring rows in
+// any column (for the shared-memory staging size).
+void ring_shape(long ng, double lo, double hi, int *jcols, int *rows_max)
+{
+    long J = std::min<long>(ng / 3, (long)ceil(hi));
+    long A = (long)ceil(hi) - 1;
+    long ia_min = std::max(-A, -ng / 2 + 1), ia_max = std::min(A, ng / 2);
+    int best = 0;
+    for (long j = 0; j < J; ++j) {
+        int n = 0;
+        for (long ia = ia_min; ia <= ia_max; ++ia) {
+            double uu = sqrt(1.0 * (double)(ia * ia + j * j));
+            if (uu >= lo && uu < hi && uu > 0.0) ++n;
+        }
+        best = std::max(best, n);
+    }
+    *jcols = (int)std::max<long>(J, 0);
+    *rows_max = best;
+}
+
+}  // namespace
+
+int build_maps(amber_cuda_ctx *c, const MapJob &job)
+{
+    const long ng = job.ng;
+    std::vector<int> jc(job.nslots);
+    int jmax = 1, rows_max = 1;
+    for (int s = 0; s < job.nslots; ++s) {
+        int rm;
+        ring_shape(ng, job.lo[s], job.hi[s], &jc[s], &rm);
+        jmax = std::max(jmax, jc[s]);
+        rows_max = std::max(rows_max, rm);
+    }
+    const double2 *tw;
+    int rc = twiddle_table(c, ng, &tw);
+    if (rc) return rc;
+    // device copies of lo/hi and column counts
+    size_t meta = sizeof(double) * 2 * job.nslots + sizeof(int) * job.nslots;
+    if ((rc = ensure(c, c->ring_lohi, meta, "ring metadata"))) return rc;
+    std::vector<unsigned char> hbuf(meta);
+    for (int s = 0; s < job.nslots; ++s) {
+        reinterpret_cast<double *>(hbuf.data())[2 * s] = job.lo[s];
+        reinterpret_cast<double *>(hbuf.data())[2 * s + 1] = job.hi[s];
+    }
+    memcpy(hbuf.data() + sizeof(double) * 2 * job.nslots, jc.data(), sizeof(int) * job.nslots);
+    if ((rc = cuda_check(c, cudaMemcpyAsync(c->ring_lohi.p, hbuf.data(), meta, cudaMemcpyHostToDevice, c->stream),
+                         "upload ring metadata")))
+        return rc;
+    if ((rc = cuda_check(c, cudaStreamSynchronize(c->stream), "ring metadata sync"))) return rc;
+    const double *d_lohi = reinterpret_cast<const double *>(c->ring_lohi.p);
+    const int *d_jc = reinterpret_cast<const int *>(reinterpret_cast<const unsigned char *>(c->ring_lohi.p) +
+                                                    sizeof(double) * 2 * job.nslots);
+
+    size_t ybytes = sizeof(double2) * (size_t)job.nslots * ng * jmax * job.nch;
+    if ((rc = ensure(c, c->y, ybytes, "map intermediate"))) return rc;
+    double2 *Y = reinterpret_cast<double2 *>(c->y.p);
+
+    // pass 1: choose channels per block so the staged column fits
+    const size_t smem_cap = 200 * 1024;
+    auto p1_smem = [&](int C) { return sizeof(double2) * ng + (sizeof(double2) * C + sizeof(int)) * rows_max; };
+    int C1 = 32;
+    while (C1 > 1 && p1_smem(C1) > smem_cap) C1 /= 2;
+    if (p1_smem(C1) > smem_cap) return fail(c, AMBER_ERR_ARG, "ring too wide for the column stage (%d rows)", rows_max);
+    dim3 g1(jmax, job.nslots, (unsigned)((job.nch + C1 - 1) / C1));
+    size_t s1 = p1_smem(C1);
+#define LAUNCH_COLS(CC)                                                                                        \
+    do {                                                                                                        \
+        cudaFuncSetAttribute(ring_cols_kernel<CC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s1);        \
+        ring_cols_kernel<CC><<<g1, kThreads, s1, c->stream>>>(job.src, job.src_complex ? 1 : 0, job.n1, job.nc, \
+                                                               job.chan_base, job.nch, ng, d_lohi, d_jc, jmax,  \
+                                                               tw, Y, rows_max);                                \
+    } while (0)
+    switch (C1) {
+        case 32: LAUNCH_COLS(32); break;
+        case 16: LAUNCH_COLS(16); break;
+        case 8: LAUNCH_COLS(8); break;
+        case 4: LAUNCH_COLS(4); break;
+        case 2: LAUNCH_COLS(2); break;
+        default: LAUNCH_COLS(1); break;
+    }
+#undef LAUNCH_COLS
+    if ((rc = cuda_check(c, cudaGetLastError(), "ring_cols_kernel launch"))) return rc;
+
+    // pass 2
+    auto p2_smem = [&](int C) { return sizeof(double2) * ng + sizeof(double2) * C * jmax; };
+    int C2 = 32;
+    while (C2 > 1 && p2_smem(C2) > smem_cap) C2 /= 2;
+    dim3 g2((unsigned)ng, job.nslots, (unsigned)((job.nch + C2 - 1) / C2));
+    size_t s2 = p2_smem(C2);
+#define LAUNCH_ROWS(CC)                                                                                        \
+    do {                                                                                                        \
+        cudaFuncSetAttribute(ring_rows_kernel<CC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s2);        \
+        ring_rows_kernel<CC><<<g2, kThreads, s2, c->stream>>>(Y, ng, jmax, d_jc, job.nch, tw, job.kp,          \
+                                                               job.out_f64, job.out_hi, job.out_lo, job.out_f32); \
+    } while (0)
+    switch (C2) {
+        case 32: LAUNCH_ROWS(32); break;
+        case 16: LAUNCH_ROWS(16); break;
+        case 8: LAUNCH_ROWS(8); break;
+        case 4: LAUNCH_ROWS(4); break;
+        case 2: LAUNCH_ROWS(2); break;
+        default: LAUNCH_ROWS(1); break;
+    }
+#undef LAUNCH_ROWS
+    return cuda_check(c, cudaGetLastError(), "ring_rows_kernel launch");
+}
+
+}  // namespace amber

@@ -1,0 +1,139 @@
+/*
+ * libamber_cuda — B200 (sm_100a) implementation of the AMBER estimator hot
+ * path behind a plain C ABI: no CUDA or torch types in any signature, host
+ * pointers and sizes only.  A C driver (amber_gpu) links it as a drop-in for
+ * the per-triangle loop of 4_fbe/amber.c and 4_fbe/amber_v2.c, and the
+ * Python package loads it with ctypes.
+ *
+ * Ownership: the context owns every device allocation; host buffers always
+ * belong to the caller.  One context per host thread; calls on one context
+ * are not re-entrant.  Every call returns AMBER_OK (0) or a negative status
+ * and never exits the process; amber_cuda_last_error() explains the last
+ * failure.  All calls are synchronous from the caller's point of view.
+ */
+#ifndef AMBER_CUDA_H
+#define AMBER_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define AMBER_API __attribute__((visibility("default")))
+#else
+#define AMBER_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define AMBER_OK 0
+#define AMBER_ERR_ARG (-1)      /* bad argument (size, range, NULL) */
+#define AMBER_ERR_OOM (-2)      /* device allocation failed or over the HBM budget */
+#define AMBER_ERR_CUDA (-3)     /* CUDA runtime or kernel launch error */
+#define AMBER_ERR_TIMEOUT (-4)  /* a bounded device-side wait gave up */
+#define AMBER_ERR_OVERFLOW (-5) /* a count does not fit the output type (v1 numdnu is int32) */
+#define AMBER_ERR_STATE (-6)    /* call order: grid / rings / channels not set yet */
+#define AMBER_ERR_NODEV (-7)    /* no usable sm_100 device: the library has no CPU fallback */
+
+/* ---- precision of the triple-product contraction ---- */
+#define AMBER_PREC_FP64 0  /* plain FP64 restatement of the reference loop (CUDA cores) */
+#define AMBER_PREC_MIXED 1 /* split-BF16×3 tcgen05/TMEM contraction, FP32 tiles, FP64 lag reduction */
+
+typedef struct amber_cuda_ctx amber_cuda_ctx;
+
+typedef struct amber_cuda_opts {
+    int device;            /* CUDA device ordinal */
+    int precision;         /* AMBER_PREC_FP64 or AMBER_PREC_MIXED */
+    size_t hbm_budget;     /* max device bytes the context may hold; 0 = 90 % of free memory */
+    void *stream;          /* optional cudaStream_t to launch on (NULL = the context's own stream) */
+    int chunk_px;          /* mixed path: pixels per FP32 accumulation chunk before the FP64 flush (0 = default) */
+} amber_cuda_opts;
+
+AMBER_API void amber_cuda_default_opts(amber_cuda_opts *opts);
+AMBER_API int amber_cuda_create(const amber_cuda_opts *opts, amber_cuda_ctx **out);
+AMBER_API void amber_cuda_destroy(amber_cuda_ctx *ctx);
+AMBER_API const char *amber_cuda_last_error(const amber_cuda_ctx *ctx);
+
+/* ---- grid input: replaces initialize + ReadGVnAC_gridding + normalize_data
+ * (4_fbe/amber_funcs.c:1720-1779, 1861-1941, 1946-1978).  The summed grid and
+ * the sampling counts are uploaded and normalised on the device:
+ * GV /= NTiG where NTiG > 0, then NTiG := 1 there.
+ * Packed form: re_im[(cell·nc + ch)·2 + {0,1}], ntig[cell·nc + ch] with
+ * cell = ii·(N1/2+1) + jj — exactly the order of the GV_data / sampling files.
+ * Pointer-per-cell form: the reference's own double** arrays
+ * (amber_funcs.c:1756-1769), GVre[cell][ch] etc. */
+AMBER_API int amber_cuda_load_grid_packed(amber_cuda_ctx *ctx, long N1, long nc, double Du, int flag_key,
+                                const double *re_im, const double *ntig);
+AMBER_API int amber_cuda_load_grid(amber_cuda_ctx *ctx, long N1, long nc, double Du, int flag_key,
+                         const double *const *GVre, const double *const *GVim, const double *const *NTiG);
+
+/* ---- ring edges: replaces annular_rings (amber_funcs.c:2022-2094).  Uavg is
+ * computed as in amber_funcs.c:2065.  Rings must lie inside the grid
+ * (UHigh ≤ N1/2), otherwise the reference would index outside it. */
+AMBER_API int amber_cuda_set_rings(amber_cuda_ctx *ctx, int Nr, const double *ULow, const double *UHigh);
+AMBER_API int amber_cuda_get_uavg(const amber_cuda_ctx *ctx, double *Uavg);
+
+/* ---- channels: replaces get_uf_chans + precompute_unflg_vcp /
+ * precompute_vcp_dnu (amber_funcs.c:2485-2508, 2207-2259, 2264-2310).
+ * uf_nc == 0 means flag_key 0 (every channel 0..nc-1).  Channels listed more
+ * than once count with their multiplicity, as in the reference's tables.
+ * Out-of-range channels are rejected. */
+AMBER_API int amber_cuda_set_channels(amber_cuda_ctx *ctx, int nc10, int uf_nc, const int *uf_chans);
+
+/* ---- closed triangles and their normaliser: replaces calCR + read_rings
+ * (amber_funcs.c:389-545).  rdata[4·t] = {r1, r2, r3, Num}, caller-owned,
+ * room for max_tri rows; *rcount receives the full count (may exceed max_tri). */
+AMBER_API int amber_cuda_calcr(amber_cuda_ctx *ctx, int max_tri, int *rcount, double *rdata);
+
+/* Padded map side of a triangle whose largest ring is r1 (amber.c:193-197). */
+AMBER_API long amber_cuda_ng1(const amber_cuda_ctx *ctx, int r1);
+
+/* ---- one triangle, file-ready: replaces the body of the rp loop,
+ * amber.c:189-304 (v1) and amber_v2.c:189-309 (v2): fill_s2d_float ×3
+ * (+ fill_s2I ×3), the OpenMP triple-product loop and the writer's scalars.
+ * bldnu / numdnu: caller-owned nclen² arrays (nclen = 2·nc10 + 1), row
+ * Δ2 + nc10, column Δ3 + nc10.  rdata_num is rdata[4·rp + 3] from calcr.
+ * v1: *Ntri = Num/Ng1², *Num = (Ng1/N1)²·rdata_num; numdnu counts the channel
+ * triplets exactly (AMBER_ERR_OVERFLOW if one exceeds INT32_MAX).
+ * v2: numdnu = Σ I_r1·I_r2·I_r3 of the ring-masked sampling maps. */
+AMBER_API int amber_cuda_triangle_v1(amber_cuda_ctx *ctx, int r1, int r2, int r3, double rdata_num, float *bldnu,
+                           int32_t *numdnu, double *Ntri, double *Num);
+AMBER_API int amber_cuda_triangle_v2(amber_cuda_ctx *ctx, int r1, int r2, int r3, float *bldnu, float *numdnu,
+                           double *inv_Ng1_Ng2);
+
+/* ---- many triangles in one call (the whole rp range of amber.c:187), FP64
+ * results before the float cast of the file writer.  tri[3·t] = {r1, r2, r3}.
+ * Triangles are grouped by r1 so each ring map is built once per map size.
+ * bldnu[t·nclen² + …]; numdnu (int64, may be NULL); numtri (v2 mask
+ * products, NULL unless want_v2).  Results are identical to calling the
+ * per-triangle form in any order. */
+AMBER_API int amber_cuda_triangles(amber_cuda_ctx *ctx, int ntri, const int *tri, int want_v2, double *bldnu,
+                         int64_t *numdnu, double *numtri);
+
+/* Split form for callers that time the device work alone: _run leaves the
+ * results on the device, _fetch copies them to the caller's buffers. */
+AMBER_API int amber_cuda_triangles_run(amber_cuda_ctx *ctx, int ntri, const int *tri, int want_v2);
+AMBER_API int amber_cuda_triangles_fetch(amber_cuda_ctx *ctx, double *bldnu, int64_t *numdnu, double *numtri);
+
+/* Lag-triple products of the last run (Σ over triangles of total_vcp·Ng1²,
+ * the reference's own per-triangle work) and its device time in ms. */
+AMBER_API int amber_cuda_last_run_stats(const amber_cuda_ctx *ctx, double *products, double *device_ms);
+
+/* ---- gridding: replaces group_loop_gridding / _without_flag
+ * (3_vcg/tgefuncs.c:377-505, 511-621).  randpar[g·npar + {0,1}] = u/ν0, v/ν0
+ * (float, as read from the random-groups parameters); data[g][ch][stokes][3]
+ * = (re, im, wt) float; only Stokes 0 (RR) is gridded, as in the files the
+ * reference writes.  Records are sorted by cell (stable, by record index) and
+ * each cell is summed in record order, so the FP64 sums are bit-identical to
+ * the reference's sequential loop.  Outputs are the summed grid and the
+ * counts in file order (caller-owned: NN·(NN/2+1)·nc·2 and ·1 doubles). */
+AMBER_API int amber_cuda_grid_vis(amber_cuda_ctx *ctx, long NN, long nc, double dU, double Umax, float nu_chan0, int flag_key,
+                        long ngroups, long npar, long nstokes, const float *randpar, const float *data,
+                        double *re_im_out, double *ntig_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

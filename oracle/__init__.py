@@ -1,0 +1,253 @@
+"""ORACLE / TEST INFRASTRUCTURE ONLY.
+
+CPU checker for the estimator path.  Only tests/, ``__graft_entry__.smoke()``
+and bench.py's CPU-baseline leg use this package; the product
+(``amber_b200`` / libamber_cuda) never imports it.
+
+* ``liboracle.so`` — our FP64 C restatement (``amber_oracle.c``), wrapped
+  below with numpy arrays;
+* ``_ref/`` — the reference's own C sources built unchanged against our FFTW
+  shim (``Makefile``): ``ref_amber`` (as shipped, float), ``ref_amber_fast``
+  (production flags, float), ``ref_amber64`` (``-Dfloat=double``) and
+  ``ref_vcg`` (gridding stage).  :func:`run_ref_amber` / :func:`run_ref_vcg`
+  drive them through files, exactly as the reference is used.
+"""
+from __future__ import annotations
+
+import ctypes
+import json
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(HERE, "_ref")
+_lib = None
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_fp = ctypes.POINTER(ctypes.c_float)
+_ip = ctypes.POINTER(ctypes.c_int)
+_i64p = ctypes.POINTER(ctypes.c_int64)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        path = os.path.join(HERE, "liboracle.so")
+        if not os.path.exists(path):
+            subprocess.run(["make", "-C", HERE, "oracle"], check=True, capture_output=True)
+        L = ctypes.CDLL(path)
+        L.orc_grid_vis.restype = ctypes.c_int
+        L.orc_grid_vis.argtypes = [ctypes.c_long, ctypes.c_long, ctypes.c_double, ctypes.c_double, ctypes.c_float,
+                                   ctypes.c_int, ctypes.c_long, ctypes.c_long, ctypes.c_long, _fp, _fp, _dp, _dp]
+        L.orc_normalize.argtypes = [ctypes.c_long, ctypes.c_long, _dp, _dp]
+        L.orc_uavg.argtypes = [ctypes.c_int, _dp, _dp, _dp]
+        L.orc_triangles.restype = ctypes.c_int
+        L.orc_triangles.argtypes = [ctypes.c_int, _dp, _ip, ctypes.c_int]
+        L.orc_ng1.restype = ctypes.c_long
+        L.orc_ng1.argtypes = [ctypes.c_double, ctypes.c_double]
+        L.orc_calcr.restype = ctypes.c_int
+        L.orc_calcr.argtypes = [ctypes.c_long, ctypes.c_long, _dp, ctypes.c_int, _dp, _dp, _dp, _dp, ctypes.c_int,
+                                ctypes.c_int]
+        for f in (L.orc_ring_map, L.orc_ring_mask_map):
+            f.restype = ctypes.c_int
+            f.argtypes = [ctypes.c_long, ctypes.c_long, _dp, ctypes.c_double, ctypes.c_double, ctypes.c_long,
+                          ctypes.c_int, _dp, ctypes.c_int]
+        L.orc_triangle.restype = ctypes.c_long
+        L.orc_triangle.argtypes = [ctypes.c_long, ctypes.c_long, ctypes.c_int, ctypes.c_int, _ip, _dp, _dp, _dp,
+                                   _dp, _dp, _dp, _dp, _i64p, _dp, ctypes.c_int]
+        L.orc_triangle_absscale.argtypes = [ctypes.c_long, ctypes.c_long, ctypes.c_int, ctypes.c_int, _ip, _dp,
+                                            _dp, _dp, _dp, ctypes.c_int]
+        _lib = L
+    return _lib
+
+
+def _p(a, t):
+    return a.ctypes.data_as(t) if a is not None else None
+
+
+NTHREADS = max(1, min(8, os.cpu_count() or 1))
+
+
+def grid_vis(nn, nc, du, umax, nu_chan0, flag_key, randpar, data):
+    """Gridding restatement; returns (re_im complex128 [NN, H, nc], ntig [NN, H, nc])."""
+    randpar = np.ascontiguousarray(randpar, dtype=np.float32)
+    data = np.ascontiguousarray(data, dtype=np.float32)
+    g, npar = randpar.shape
+    nstokes = data.shape[2]
+    h = nn // 2 + 1
+    re_im = np.zeros((nn, h, nc, 2), dtype=np.float64)
+    ntig = np.zeros((nn, h, nc), dtype=np.float64)
+    rc = lib().orc_grid_vis(nn, nc, du, umax, np.float32(nu_chan0), flag_key, g, npar, nstokes, _p(randpar, _fp),
+                            _p(data, _fp), _p(re_im, _dp), _p(ntig, _dp))
+    if rc != 0:
+        raise ValueError("record outside the grid")
+    return re_im[..., 0] + 1j * re_im[..., 1], ntig
+
+
+def normalize(gv, counts):
+    re_im = np.ascontiguousarray(np.stack([gv.real, gv.imag], axis=-1))
+    ntig = np.ascontiguousarray(counts, dtype=np.float64).copy()
+    nn, h, nc = counts.shape
+    lib().orc_normalize(nn * h, nc, _p(re_im, _dp), _p(ntig, _dp))
+    return re_im[..., 0] + 1j * re_im[..., 1], ntig
+
+
+def uavg(ulow, uhigh):
+    lo = np.ascontiguousarray(ulow, dtype=np.float64)
+    hi = np.ascontiguousarray(uhigh, dtype=np.float64)
+    out = np.zeros_like(lo)
+    lib().orc_uavg(len(lo), _p(lo, _dp), _p(hi, _dp), _p(out, _dp))
+    return out
+
+
+def triangles(ulow, uhigh):
+    ua = uavg(ulow, uhigh)
+    n = lib().orc_triangles(len(ua), _p(ua, _dp), None, 0)
+    tri = np.zeros((max(n, 1), 3), dtype=np.int32)
+    lib().orc_triangles(len(ua), _p(ua, _dp), _p(tri, _ip), n)
+    return tri[:n]
+
+
+def ng1(uhigh, du):
+    return int(lib().orc_ng1(float(uhigh), float(du)))
+
+
+def calcr(ntig_norm, ulow, uhigh):
+    nn, h, nc = ntig_norm.shape
+    lo = np.ascontiguousarray(ulow, dtype=np.float64)
+    hi = np.ascontiguousarray(uhigh, dtype=np.float64)
+    ua = uavg(lo, hi)
+    maxtri = int(lib().orc_triangles(len(ua), _p(ua, _dp), None, 0))
+    rdata = np.zeros((max(maxtri, 1), 4), dtype=np.float64)
+    nt = np.ascontiguousarray(ntig_norm, dtype=np.float64)
+    n = lib().orc_calcr(nn, nc, _p(nt, _dp), len(lo), _p(lo, _dp), _p(hi, _dp), _p(ua, _dp), _p(rdata, _dp),
+                        maxtri, NTHREADS)
+    return rdata[:n]
+
+
+def ring_maps(gv_norm, lo, hi, ng, mask=False, channels=None):
+    """FP64 maps [nc][Ng1·Ng1] of one ring (all channels, or the listed ones)."""
+    nn, h, nc = gv_norm.shape
+    if mask:
+        src = np.ascontiguousarray(gv_norm, dtype=np.float64)
+    else:
+        src = np.ascontiguousarray(np.stack([gv_norm.real, gv_norm.imag], axis=-1))
+    out = np.zeros((nc, ng * ng), dtype=np.float64)
+    fn = lib().orc_ring_mask_map if mask else lib().orc_ring_map
+    for p in (range(nc) if channels is None else channels):
+        row = np.zeros(ng * ng, dtype=np.float64)
+        rc = fn(nn, nc, _p(src, _dp), float(lo), float(hi), ng, int(p), _p(row, _dp), 1)
+        if rc != 0:
+            raise ValueError("ring reaches outside the grid")
+        out[p] = row
+    return out
+
+
+def triangle(m1, m2, m3, nc10, uf_chans=None, i1=None, i2=None, i3=None):
+    """FP64 lag accumulation; returns (bldnu [nclen,nclen], numdnu int64, numtri or None, total_vcp)."""
+    nc, k = m1.shape
+    nclen = 2 * nc10 + 1
+    uf = None if uf_chans is None else np.ascontiguousarray(uf_chans, dtype=np.int32)
+    bl = np.zeros(nclen * nclen)
+    nd = np.zeros(nclen * nclen, dtype=np.int64)
+    nt = np.zeros(nclen * nclen) if i1 is not None else None
+    arrs = [np.ascontiguousarray(a, dtype=np.float64) if a is not None else None for a in (m1, m2, m3, i1, i2, i3)]
+    tot = lib().orc_triangle(k, nc, nc10, 0 if uf is None else len(uf), _p(uf, _ip), *[_p(a, _dp) for a in arrs],
+                             _p(bl, _dp), _p(nd, _i64p), _p(nt, _dp), NTHREADS)
+    return (bl.reshape(nclen, nclen), nd.reshape(nclen, nclen),
+            None if nt is None else nt.reshape(nclen, nclen), int(tot))
+
+
+def triangle_absscale(m1, m2, m3, nc10, uf_chans=None):
+    nc, k = m1.shape
+    nclen = 2 * nc10 + 1
+    uf = None if uf_chans is None else np.ascontiguousarray(uf_chans, dtype=np.int32)
+    out = np.zeros(nclen * nclen)
+    arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (m1, m2, m3)]
+    lib().orc_triangle_absscale(k, nc, nc10, 0 if uf is None else len(uf), _p(uf, _ip), *[_p(a, _dp) for a in arrs],
+                                _p(out, _dp), NTHREADS)
+    return out.reshape(nclen, nclen)
+
+
+def estimate(real, version=1, tri_subset=None, with_absscale=False):
+    """Full FP64 oracle pass over a synth.Realisation: normalise, calCR,
+    then per closed triangle maps + lag accumulation.  Returns a list of dicts
+    in calCR order (optionally restricted to ``tri_subset`` indices)."""
+    gvn, ntn = normalize(real.gv, real.counts)
+    rdata = calcr(ntn, real.ulow, real.uhigh)
+    uf = real.uf_chans if real.flag_key == 1 else None
+    out = []
+    idxs = range(len(rdata)) if tri_subset is None else tri_subset
+    for t in idxs:
+        r1, r2, r3 = (int(v) for v in rdata[t, :3])
+        ng = ng1(real.uhigh[r1], real.du)
+        m = [ring_maps(gvn, real.ulow[r], real.uhigh[r], ng) for r in (r1, r2, r3)]
+        im = [ring_maps(ntn, real.ulow[r], real.uhigh[r], ng, mask=True) for r in (r1, r2, r3)] if version == 2 \
+            else [None] * 3
+        bl, nd, nt, tot = triangle(*m, real.nc10, uf, *im)
+        rec = dict(rp=t, r1=r1, r2=r2, r3=r3, ng1=ng, rdata_num=float(rdata[t, 3]), bldnu=bl, numdnu=nd,
+                   numtri=nt, total_vcp=tot)
+        if with_absscale:
+            rec["absscale"] = triangle_absscale(*m, real.nc10, uf)
+            if version == 2:
+                rec["absscale_i"] = triangle_absscale(*im, real.nc10, uf)
+        out.append(rec)
+    return rdata, out
+
+
+# ---- the reference's own code, built from its sources (oracle/_ref) -------------------------
+
+def ref_available():
+    return all(os.path.exists(os.path.join(REF_DIR, b)) for b in ("ref_amber", "ref_amber64", "ref_vcg"))
+
+
+def run_ref_amber(real, workdir, version=1, fp64=False, fast=False, rp_begin=0, rp_end=-1, nthreads=None,
+                  rlzn=1):
+    """Write ``real`` as amber input files under ``workdir`` and run the
+    reference build.  Returns (json_stats, res_path)."""
+    from amber_b200 import formats  # local import: formats is a plain file-format module
+    data_path = os.path.join(workdir, "data")
+    res_path = os.path.join(workdir, "res")
+    os.makedirs(res_path, exist_ok=True)
+    real.write(data_path, rlzn)
+    params = os.path.join(workdir, "input_params_ess")
+    formats.write_input_params_ess(params, 154.255e6, 40.0e3, 1.0, data_path)
+    rings = os.path.join(workdir, "rings.txt")
+    formats.write_rings_file(rings, real.ulow, real.uhigh)
+    exe = "ref_amber64" if fp64 else ("ref_amber_fast" if fast else "ref_amber")
+    uf_nc = len(real.uf_chans) if real.flag_key == 1 else 0
+    cmd = [os.path.join(REF_DIR, exe), str(rlzn), "v2" if version == 2 else "v1", str(real.nc10), str(uf_nc), rings,
+           str(rp_begin), str(rp_end), str(nthreads or NTHREADS), res_path, params]
+    p = subprocess.run(cmd, capture_output=True, text=True, cwd=workdir)
+    if p.returncode != 0:
+        raise RuntimeError(f"{exe} failed: {p.stderr[-2000:]}")
+    line = [ln for ln in p.stdout.splitlines() if ln.startswith("AMBER_REF_JSON ")][-1]
+    return json.loads(line[len("AMBER_REF_JSON "):]), res_path
+
+
+def run_ref_vcg(randpar, data, nu_chan0, nc, umax, fwhm, flag_key, workdir):
+    """Run the reference's own gridding stage (3_vcg main + tgefuncs) on
+    synthetic records; returns (gv complex [NN,H,nc], ntig, dU, NN)."""
+    from amber_b200 import formats
+    vis = os.path.join(workdir, "vis.bin")
+    formats.write_vis(vis, randpar, data, nu_chan0, 40.0e3, 1.0)
+    params = os.path.join(workdir, "inputparameters")
+    with open(params, "w") as f:
+        f.write(f"{nc}\t{umax!r}\t{fwhm!r}\t1.\n")
+    gvp = os.path.join(workdir, "GV_out")
+    smp = os.path.join(workdir, "sampling_out")
+    p = subprocess.run([os.path.join(REF_DIR, "ref_vcg"), vis, params, gvp, str(flag_key), "0", "1", smp],
+                       capture_output=True, text=True, cwd=workdir)
+    if p.returncode != 0:
+        raise RuntimeError(f"ref_vcg failed: {p.stdout[-1000:]} {p.stderr[-1000:]}")
+    gv, du, fk = formats.read_gv(gvp)
+    nn = gv.shape[0]
+    ntig = formats.read_sampling(smp, nn, gv.shape[2])
+    return gv, ntig, du, nn
+
+
+def tmpdir():
+    return tempfile.mkdtemp(prefix="amber_oracle_")

@@ -1,0 +1,98 @@
+"""Regenerate the golden fixtures in this folder from the REFERENCE's own code.
+
+Runs oracle/_ref/ref_amber64 (4_fbe/amber_funcs.c + vars.c built unchanged
+with -Dfloat=double), ref_amber (as shipped, float) and ref_vcg (3_vcg/main.c +
+tgefuncs.c unchanged) on small seeded synthetic inputs and stores inputs and
+outputs as compressed .npz files:
+
+  est_<name>.npz   — grid sums, counts, ring edges, nc10, channels, and the
+                     reference's closed_rings plus, per triangle, its v1
+                     (FP64 and float builds) and v2 (FP64) lag arrays;
+  grid_<name>.npz  — visibility records and the reference's GV/sampling sums.
+
+Needs the reference sources (make -C oracle ref); run from the repo root:
+    python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+import oracle  # noqa: E402
+from amber_b200 import formats, synth  # noqa: E402
+
+OUT = os.path.dirname(os.path.abspath(__file__))
+
+EST_CASES = {
+    # name: (nn, nc, seed, nbins, hi, nc10, flagged)
+    "unflagged32": (32, 8, 3, 4, 14.0, 3, None),
+    "flagged48": (48, 12, 4, 5, 21.0, 5, [0, 5, 11]),
+    "dup40": (40, 10, 6, 4, 18.0, 6, None),  # uf_chans with a repeated channel, see below
+}
+
+
+def est_case(name, nn, nc, seed, nbins, hi, nc10, flagged):
+    real = synth.tiny(nn, nc, seed=seed, nbins=nbins, hi=hi, nc10=nc10, flagged=flagged)
+    if name == "dup40":
+        real.flag_key = 1
+        real.uf_chans = np.array([0, 1, 2, 3, 3, 5, 6, 8, 9], dtype=np.int32)  # channel 3 twice, 4 and 7 absent
+    nclen = real.nclen
+    rec = dict(gv=real.gv, counts=real.counts, ulow=real.ulow, uhigh=real.uhigh, nc10=real.nc10,
+               uf_chans=real.uf_chans, flag_key=real.flag_key, du=real.du)
+    st64, rp64 = oracle.run_ref_amber(real, oracle.tmpdir(), version=1, fp64=True)
+    rdata = formats.read_closed_rings(rp64)
+    rec["rdata"] = rdata
+    st32, rp32 = oracle.run_ref_amber(real, oracle.tmpdir(), version=1, fp64=False)
+    sv2, rpv2 = oracle.run_ref_amber(real, oracle.tmpdir(), version=2, fp64=True)
+    b64, n64, b32, ntri, num, bv2, nv2, inv = [], [], [], [], [], [], [], []
+    for r1, r2, r3, _ in rdata:
+        r1, r2, r3 = int(r1), int(r2), int(r3)
+        t, nu, bl, nd = formats.read_bsout_v1(os.path.join(rp64, formats.bsout_name(1, r1, r2, r3, 1)), nclen,
+                                              np.float64)
+        b64.append(bl); n64.append(nd); ntri.append(t); num.append(nu)
+        _, _, bl32, nd32 = formats.read_bsout_v1(os.path.join(rp32, formats.bsout_name(1, r1, r2, r3, 1)), nclen)
+        assert (nd32 == nd).all()
+        b32.append(bl32)
+        iv, blv, ndv = formats.read_bsout_v2(os.path.join(rpv2, formats.bsout_name(2, r1, r2, r3, 1)), nclen,
+                                             np.float64)
+        bv2.append(blv); nv2.append(ndv); inv.append(iv)
+    rec.update(bldnu64=np.array(b64), numdnu=np.array(n64), bldnu32=np.array(b32), ntri=np.array(ntri),
+               num=np.array(num), bldnu_v2=np.array(bv2), numtri_v2=np.array(nv2), inv_ng=np.array(inv),
+               total_vcp=st64["total_vcp"])
+    np.savez_compressed(os.path.join(OUT, f"est_{name}.npz"), **rec)
+    print(name, "triangles", len(rdata), "total_vcp", st64["total_vcp"])
+
+
+GRID_CASES = {
+    # name: (nc, ngroups, seed, flag_key, fwhm_arcmin, umax_wavelengths)
+    "flag1": (5, 2000, 11, 1, 1480.73, 30.0),
+    "flag0": (4, 1200, 12, 0, 1480.73, 25.0),
+}
+
+
+def grid_case(name, nc, ngroups, seed, flag_key, fwhm, umax):
+    # dU the reference derives from the beam (tgefuncs.c:306-309)
+    import math
+    theta0 = 0.6 * fwhm * math.pi / (180. * 60.)
+    du = math.sqrt(math.log(2)) / (math.pi * theta0)
+    nn = 2 * int(math.ceil(umax / du))
+    randpar, data = synth.make_visibilities(nn, du, nc, ngroups, seed, umax=umax * 1.02)
+    gv, ntig, du_ref, nn_ref = oracle.run_ref_vcg(randpar, data, np.float32(synth.NU0), nc, umax, fwhm, flag_key,
+                                                  oracle.tmpdir())
+    np.savez_compressed(os.path.join(OUT, f"grid_{name}.npz"), randpar=randpar, data=data, nu0=np.float32(synth.NU0),
+                        du=du_ref, nn=nn_ref, umax=umax, flag_key=flag_key, gv=gv, ntig=ntig)
+    print(name, "NN", nn_ref, "dU", du_ref, "cells hit", int((ntig.sum(axis=2) > 0).sum()))
+
+
+if __name__ == "__main__":
+    if not oracle.ref_available():
+        raise SystemExit("build the reference first: make -C oracle ref")
+    for k, v in EST_CASES.items():
+        est_case(k, *v)
+    for k, v in GRID_CASES.items():
+        grid_case(k, *v)

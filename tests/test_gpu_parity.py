@@ -1,0 +1,169 @@
+"""Parity of libamber_cuda against the oracle and the reference's own outputs.
+
+Tolerances (from the contract of this path):
+* FP64 plain path: ≤ 1e-10 relative to Σ|products| per lag cell vs the FP64
+  oracle (and the reference's FP64 build via the golden fixtures);
+* mixed-precision path: ≤ 1e-6 relative to Σ|products| per lag cell;
+* triplet counts, the closed-triangle list and gridding: bit-exact.
+"""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from amber_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+TOL64 = 1e-10
+TOLMIX = 1e-6
+
+
+def _real_from(z):
+    return synth.Realisation(nn=z["gv"].shape[0], nc=z["gv"].shape[2], du=float(z["du"]), flag_key=int(z["flag_key"]),
+                             gv=z["gv"], counts=z["counts"], uf_chans=z["uf_chans"], ulow=z["ulow"],
+                             uhigh=z["uhigh"], nc10=int(z["nc10"]), seed=0)
+
+
+@pytest.fixture(scope="module")
+def lib_built():
+    from amber_b200 import build
+    build.build()
+    return True
+
+
+def _run(real, precision, version, est_cls):
+    from amber_b200 import estimate, Estimator
+    return estimate(real, precision=precision, version=version)
+
+
+@pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLDEN, "est_*.npz"))))
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_estimator_vs_reference_golden(path, precision, lib_built):
+    import amber_b200
+    z = np.load(path)
+    real = _real_from(z)
+    rdata, res = amber_b200.estimate(real, precision=precision, version=2)
+    _, ores = oracle.estimate(real, version=2, with_absscale=True)
+    np.testing.assert_array_equal(rdata[:, :3], z["rdata"][:, :3])
+    np.testing.assert_allclose(rdata[:, 3], z["rdata"][:, 3], rtol=1e-10, atol=1e-10 * np.abs(z["rdata"][:, 3]).max())
+    tol = TOL64 if precision == "fp64" else TOLMIX
+    for i, r in enumerate(res):
+        np.testing.assert_array_equal(r["numdnu"], z["numdnu"][i])
+        e = np.abs(r["bldnu"] - z["bldnu64"][i]) / (ores[i]["absscale"] + 1e-300)
+        assert e.max() <= tol, (i, e.max())
+        ei = np.abs(r["numtri"] - z["numtri_v2"][i]) / (ores[i]["absscale_i"] + 1e-300)
+        assert ei.max() <= tol, (i, ei.max())
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("nn,nc,nbins,hi,nc10,flagged,seed", [
+    (48, 16, 5, 22.0, 7, None, 31),
+    (64, 20, 6, 30.0, 9, [0, 1, 18, 19], 32),
+    (56, 12, 4, 26.0, 11, [3], 33),  # nc10 = nc - 1: the widest lag window
+])
+def test_estimator_vs_oracle(precision, nn, nc, nbins, hi, nc10, flagged, seed, lib_built):
+    import amber_b200
+    real = synth.tiny(nn, nc, seed=seed, nbins=nbins, hi=hi, nc10=nc10, flagged=flagged)
+    rdata, res = amber_b200.estimate(real, precision=precision, version=2)
+    ordata, ores = oracle.estimate(real, version=2, with_absscale=True)
+    np.testing.assert_array_equal(rdata[:, :3], ordata[:, :3])
+    tol = TOL64 if precision == "fp64" else TOLMIX
+    for r, o in zip(res, ores):
+        np.testing.assert_array_equal(r["numdnu"], o["numdnu"])
+        e = np.abs(r["bldnu"] - o["bldnu"]) / (o["absscale"] + 1e-300)
+        assert e.max() <= tol, e.max()
+        ei = np.abs(r["numtri"] - o["numtri"]) / (o["absscale_i"] + 1e-300)
+        assert ei.max() <= tol, ei.max()
+
+
+def test_triangle_v1_v2_file_scalars(lib_built):
+    import amber_b200
+    z = np.load(os.path.join(GOLDEN, "est_flagged48.npz"))
+    real = _real_from(z)
+    with amber_b200.Estimator(precision="fp64") as est:
+        est.load_grid(real.gv, real.counts, real.du, real.flag_key)
+        est.set_rings(real.ulow, real.uhigh)
+        est.set_channels(real.nc10, real.uf_chans)
+        rdata = est.calcr()
+        for rp in (0, len(rdata) // 2, len(rdata) - 1):
+            r1, r2, r3 = (int(v) for v in rdata[rp, :3])
+            ntri, num, bl, nd = est.triangle_v1(r1, r2, r3, rdata[rp, 3])
+            np.testing.assert_allclose(num, z["num"][rp], rtol=1e-10)
+            np.testing.assert_allclose(ntri, z["ntri"][rp], rtol=1e-10)
+            assert nd.dtype == np.int32 and np.array_equal(nd, z["numdnu"][rp])
+            assert np.abs(bl - z["bldnu64"][rp]).max() <= 1e-6 * np.abs(z["bldnu64"][rp]).max()
+            inv, bl2, nd2 = est.triangle_v2(r1, r2, r3)
+            assert inv == z["inv_ng"][rp]
+            assert nd2.dtype == np.float32
+
+
+def test_pointer_per_cell_load_equals_packed(lib_built):
+    import amber_b200
+    real = synth.tiny(32, 8, seed=5, nbins=4, hi=14.0, nc10=3)
+    outs = []
+    for form in ("packed", "cells"):
+        with amber_b200.Estimator(precision="fp64") as est:
+            if form == "packed":
+                est.load_grid(real.gv, real.counts, real.du, real.flag_key)
+            else:
+                est.load_grid_cells(real.gv, real.counts, real.du, real.flag_key)
+            est.set_rings(real.ulow, real.uhigh)
+            est.set_channels(real.nc10)
+            rdata = est.calcr()
+            outs.append(est.triangles(rdata[:, :3].astype(np.int32))[0])
+    assert np.array_equal(outs[0], outs[1])
+
+
+@pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLDEN, "grid_*.npz"))))
+def test_gridding_bit_exact_vs_reference(path, lib_built):
+    import amber_b200
+    z = np.load(path)
+    with amber_b200.Estimator(precision="fp64") as est:
+        gv, nt = est.grid_vis(int(z["nn"]), z["gv"].shape[2], float(z["du"]), float(z["umax"]), z["nu0"],
+                              int(z["flag_key"]), z["randpar"], z["data"])
+    assert np.array_equal(gv.real, z["gv"].real) and np.array_equal(gv.imag, z["gv"].imag)
+    assert np.array_equal(nt, z["ntig"])
+
+
+def test_gridding_bit_exact_vs_oracle_large(lib_built):
+    import amber_b200
+    nn, du, nc = 128, 0.5, 24
+    randpar, data = synth.make_visibilities(nn, du, nc, 60000, 77, dup_frac=0.6)
+    for fk in (0, 1):
+        g_o, n_o = oracle.grid_vis(nn, nc, du, 0.95 * du * nn / 2, np.float32(synth.NU0), fk, randpar, data)
+        with amber_b200.Estimator() as est:
+            g, n = est.grid_vis(nn, nc, du, 0.95 * du * nn / 2, np.float32(synth.NU0), fk, randpar, data)
+        assert np.array_equal(g, g_o) and np.array_equal(n, n_o)
+
+
+def test_error_paths(lib_built):
+    import amber_b200
+    from amber_b200 import AmberError
+    real = synth.tiny(32, 8, seed=5, nbins=4, hi=14.0, nc10=3)
+    with amber_b200.Estimator(precision="fp64") as est:
+        with pytest.raises(AmberError) as e:
+            est.calcr()
+        assert e.value.code == -6  # no grid yet
+        est.load_grid(real.gv, real.counts, real.du, real.flag_key)
+        with pytest.raises(AmberError) as e:
+            est.set_channels(3, [0, 1, 99])
+        assert e.value.code == -1
+        with pytest.raises(AmberError):
+            est.set_channels(8)  # nc10 must be < nc
+        est.set_rings([2.0, 5.0], [5.0, 20.0])  # 20 > N1/2 = 16
+        with pytest.raises(AmberError) as e:
+            est.calcr()
+        assert e.value.code == -1
+        with pytest.raises(AmberError):
+            est.set_rings([5.0], [4.0])
+        est.set_rings(real.ulow, real.uhigh)
+        est.set_channels(3)
+        with pytest.raises(AmberError):
+            est.triangles(np.array([[0, 0, 9]], dtype=np.int32))
+        # still usable after errors
+        rd = est.calcr()
+        assert len(rd) > 0
