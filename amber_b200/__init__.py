@@ -28,7 +28,7 @@ LIB_PATH = os.path.join(HERE, "libamber_cuda.so")
 AMBER_OK = 0
 ERRORS = {-1: "bad argument", -2: "out of device memory / over budget", -3: "CUDA error", -4: "timeout",
           -5: "overflow", -6: "call order", -7: "no sm_100 device"}
-PREC = {"fp64": 0, "mixed": 1}
+PREC = {"fp64": 0, "mixed": 1, "bf16x3": 2}
 
 # every entry point include/amber_cuda.h declares
 EXPORTS = (

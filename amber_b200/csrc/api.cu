@@ -200,7 +200,8 @@ int amber_cuda_create(const amber_cuda_opts *opts, amber_cuda_ctx **out)
     amber_cuda_opts o;
     amber_cuda_default_opts(&o);
     if (opts) o = *opts;
-    if (o.precision != AMBER_PREC_FP64 && o.precision != AMBER_PREC_MIXED) return AMBER_ERR_ARG;
+    if (o.precision != AMBER_PREC_FP64 && o.precision != AMBER_PREC_MIXED && o.precision != AMBER_PREC_BF16X3)
+        return AMBER_ERR_ARG;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= o.device) {
         cudaGetLastError();
@@ -444,13 +445,15 @@ int amber_cuda_triangles_run(amber_cuda_ctx *c, int ntri, const int *tri, int wa
         }
         it->tris.push_back(t);
     }
-    const bool mixed = c->precision == AMBER_PREC_MIXED;
-    const size_t vbytes = mixed ? 4 : 8;  // per map value: hi+lo bf16, or FP64
+    const int prec = c->precision;
+    // bytes per map value: FP64; int8 path: FP32 plane + 3 digit planes; bf16 path: hi + lo
+    const size_t vbytes = prec == AMBER_PREC_FP64 ? 8 : (prec == AMBER_PREC_MIXED ? 7 : 4);
+    const long kalign = prec == AMBER_PREC_MIXED ? 128 : 64;
     c->last_products = 0;
     cudaEventRecord(c->ev0, c->stream);
     for (const Group &g : groups) {
-        const long k = g.ng * g.ng, kp = (k + 63) / 64 * 64;
-        const size_t per_slot = vbytes * (size_t)c->nc * kp;
+        const long k = g.ng * g.ng, kp = (k + kalign - 1) / kalign * kalign;
+        const size_t per_slot = vbytes * (size_t)c->nc * kp + 8 * (size_t)c->nc;
         // Process the group's triangles in batches whose ring union fits the budget.
         size_t spare = c->budget > c->held ? c->budget - c->held : 0;
         spare += c->maps_d.bytes + c->maps_i.bytes;
@@ -482,8 +485,34 @@ int amber_cuda_triangles_run(amber_cuda_ctx *c, int ntri, const int *tri, int wa
                 ms.ring_of_slot.push_back(r);
             }
             ms.nslots = (int)ms.ring_of_slot.size();
+            const size_t nvals = (size_t)ms.nslots * c->nc * kp, nrows = (size_t)ms.nslots * c->nc;
             if ((rc = ensure(c, c->maps_d, per_slot * ms.nslots, "ring maps"))) return rc;
             if (want_v2 && (rc = ensure(c, c->maps_i, per_slot * ms.nslots, "ring mask maps"))) return rc;
+            // carve one map set (D or I) out of its buffer
+            auto carve = [&](void *base, MapJob &job, DigitMaps *dm_base) {
+                char *p = (char *)base;
+                if (prec == AMBER_PREC_FP64) {
+                    job.out_f64 = (double *)p;
+                } else if (prec == AMBER_PREC_BF16X3) {
+                    job.out_hi = (uint16_t *)p;
+                    job.out_lo = (uint16_t *)p + nvals;
+                } else {
+                    job.out_f32 = (float *)p;
+                    job.d0 = (int8_t *)(p + 4 * nvals);
+                    job.d1 = job.d0 + nvals;
+                    job.d2 = job.d1 + nvals;
+                    job.expo = (int *)(p + 7 * nvals);
+                    job.rowmax = (unsigned *)(job.expo + nrows);
+                    if (dm_base) {
+                        dm_base->f32 = job.out_f32;
+                        dm_base->d0 = job.d0;
+                        dm_base->d1 = job.d1;
+                        dm_base->d2 = job.d2;
+                        dm_base->expo = job.expo;
+                    }
+                }
+            };
+            DigitMaps dmaps[2];
             for (int pass = 0; pass < (want_v2 ? 2 : 1); ++pass) {
                 MapJob job{};
                 job.src = pass == 0 ? c->grid.p : c->mask.p;
@@ -499,30 +528,39 @@ int amber_cuda_triangles_run(amber_cuda_ctx *c, int ntri, const int *tri, int wa
                     job.lo.push_back(c->ulow[r]);
                     job.hi.push_back(c->uhigh[r]);
                 }
-                void *base = pass == 0 ? c->maps_d.p : c->maps_i.p;
-                if (mixed) {
-                    job.out_hi = (uint16_t *)base;
-                    job.out_lo = (uint16_t *)base + (size_t)ms.nslots * c->nc * kp;
-                } else {
-                    job.out_f64 = (double *)base;
-                }
+                carve(pass == 0 ? c->maps_d.p : c->maps_i.p, job, &dmaps[pass]);
+                if (job.rowmax &&
+                    (rc = cuda_check(c, cudaMemsetAsync(job.rowmax, 0, sizeof(unsigned) * nrows, c->stream),
+                                     "row max reset")))
+                    return rc;
                 if ((rc = build_maps(c, job))) return rc;
             }
             for (int t : batch) {
-                int s1 = ms.slot_of_ring[tri[3 * t]], s2 = ms.slot_of_ring[tri[3 * t + 1]],
-                    s3 = ms.slot_of_ring[tri[3 * t + 2]];
+                const size_t s1 = ms.slot_of_ring[tri[3 * t]], s2 = ms.slot_of_ring[tri[3 * t + 1]],
+                             s3 = ms.slot_of_ring[tri[3 * t + 2]];
+                const size_t ss = (size_t)c->nc * kp;
                 for (int pass = 0; pass < (want_v2 ? 2 : 1); ++pass) {
                     void *base = pass == 0 ? c->maps_d.p : c->maps_i.p;
                     double *lag = res + ((size_t)t * 2 + pass) * ncsize;
-                    if (mixed) {
+                    if (prec == AMBER_PREC_MIXED) {
+                        const DigitMaps &b = dmaps[pass];
+                        auto slot = [&](size_t s) {
+                            DigitMaps d;
+                            d.f32 = b.f32 + s * ss;
+                            d.d0 = b.d0 + s * ss;
+                            d.d1 = b.d1 + s * ss;
+                            d.d2 = b.d2 + s * ss;
+                            d.expo = b.expo + s * c->nc;
+                            return d;
+                        };
+                        rc = contract_i8(c, slot(s1), slot(s2), slot(s3), k, kp, lag);
+                    } else if (prec == AMBER_PREC_BF16X3) {
                         const uint16_t *hi = (const uint16_t *)base;
-                        const uint16_t *lo = hi + (size_t)ms.nslots * c->nc * kp;
-                        const size_t ss = (size_t)c->nc * kp;
-                        rc = contract_mixed(c, hi + s1 * ss, lo + s1 * ss, hi + s2 * ss, lo + s2 * ss, hi + s3 * ss,
-                                            lo + s3 * ss, k, kp, lag);
+                        const uint16_t *lo = hi + nvals;
+                        rc = contract_bf16x3(c, hi + s1 * ss, lo + s1 * ss, hi + s2 * ss, lo + s2 * ss, hi + s3 * ss,
+                                             lo + s3 * ss, k, kp, lag);
                     } else {
                         const double *m = (const double *)base;
-                        const size_t ss = (size_t)c->nc * kp;
                         rc = contract_fp64(c, m + s1 * ss, m + s2 * ss, m + s3 * ss, k, kp, lag);
                     }
                     if (rc) return rc;

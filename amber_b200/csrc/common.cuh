@@ -107,15 +107,27 @@ struct MapJob {
     double *out_f64;
     uint16_t *out_hi, *out_lo;  // bf16 planes
     float *out_f32;
+    unsigned *rowmax;             // per (slot, channel) max |fp32 value| (zeroed by the caller)
+    int8_t *d0, *d1, *d2;         // int8 digit planes (written from out_f32 when non-null)
+    int *expo;                    // per (slot, channel) row exponent of the digits
 };
 int build_maps(amber_cuda_ctx *c, const MapJob &job);
 
 // FP64 contraction of one triangle into a lag array (device).
 int contract_fp64(amber_cuda_ctx *c, const double *m1, const double *m2, const double *m3, long k, long kp,
                   double *lag_out);
-// Mixed-precision contraction (split-BF16×3, tcgen05/TMEM).
-int contract_mixed(amber_cuda_ctx *c, const uint16_t *h1, const uint16_t *l1, const uint16_t *h2,
-                   const uint16_t *l2, const uint16_t *h3, const uint16_t *l3, long k, long kp, double *lag_out);
+// Split-BF16×3 contraction (tcgen05, FP32 accumulation in TMEM).
+int contract_bf16x3(amber_cuda_ctx *c, const uint16_t *h1, const uint16_t *l1, const uint16_t *h2,
+                    const uint16_t *l2, const uint16_t *h3, const uint16_t *l3, long k, long kp, double *lag_out);
+// Mixed-precision contraction: 3-digit int8 fixed point on the tensor cores
+// (tcgen05 kind::i8, exact int32 accumulation in TMEM).
+struct DigitMaps {
+    const float *f32;                 // [nc][kp]
+    const int8_t *d0, *d1, *d2;       // [nc][kp]
+    const int *expo;                  // [nc]
+};
+int contract_i8(amber_cuda_ctx *c, const DigitMaps &m1, const DigitMaps &m2, const DigitMaps &m3, long k, long kp,
+                double *lag_out);
 // lag[d] = Σ_u partial[u][d] (compensated, fixed order).
 int lag_reduce(amber_cuda_ctx *c, const double *partial, long nunits, long ncsize, double *lag);
 // Σ_x a·b·c over n points (FP64, deterministic) into out[0].

@@ -174,7 +174,8 @@ __global__ void __launch_bounds__(kThreads) ring_rows_kernel(const double2 *__re
                                                               double *__restrict__ out_f64,
                                                               uint16_t *__restrict__ out_hi,
                                                               uint16_t *__restrict__ out_lo,
-                                                              float *__restrict__ out_f32)
+                                                              float *__restrict__ out_f32,
+                                                              unsigned *__restrict__ rowmax)
 {
     extern __shared__ double2 smem[];
     double2 *tw = smem;       // ng
@@ -201,6 +202,7 @@ __global__ void __launch_bounds__(kThreads) ring_rows_kernel(const double2 *__re
     const int gid = warp * G + g;
     const int ngroups = (kThreads / 32) * G;
     const long slot_row = ((long)s * nch + q0 + q) * kp + n0 * ng;
+    float amax = 0.f;  // max |fp32 value| this thread writes (row exponent for the int8 digits)
     for (long nb = gid; nb * R < ng; nb += ngroups) {
         double acc[R];
         int idx[R], step[R];
@@ -230,7 +232,11 @@ __global__ void __launch_bounds__(kThreads) ring_rows_kernel(const double2 *__re
                 long o = slot_row + n1;
                 double v = acc[r];
                 if (out_f64) out_f64[o] = v;
-                if (out_f32) out_f32[o] = (float)v;
+                if (out_f32) {
+                    float f = (float)v;
+                    out_f32[o] = f;
+                    amax = fmaxf(amax, fabsf(f));
+                }
                 if (out_hi) {
                     // split: hi = bf16(v), lo = bf16(v − hi) (both round-to-nearest)
                     float f = (float)v;
@@ -241,6 +247,51 @@ __global__ void __launch_bounds__(kThreads) ring_rows_kernel(const double2 *__re
                 }
             }
         }
+    }
+    if (rowmax && q0 + q < nch) atomicMax(&rowmax[(long)s * nch + q0 + q], __float_as_uint(amax));
+}
+
+// Fixed-point digits of one map row for the int8 tensor-core contraction.
+// E is the smallest exponent with max|v| < 2^E; then, with base 254,
+//     v·2^−E·127 = d0 + d1/254 + d2/254² + r,   d0, d1, d2 ∈ [−127, 127],
+// |r| ≤ 1/(2·254²): signed, balanced digits that use the whole int8 range.
+__device__ __forceinline__ void digits254(float t, uint32_t &b0, uint32_t &b1, uint32_t &b2)
+{
+    // round-to-nearest via the 1.5·2^23 magic number: the integer sits in the
+    // low mantissa bits, so its low byte is the two's-complement int8 digit
+    const float M = 12582912.0f;
+    float y0 = t + M;
+    float r0 = (t - (y0 - M)) * 254.f;
+    float y1 = r0 + M;
+    float r1 = (r0 - (y1 - M)) * 254.f;
+    float y2 = r1 + M;
+    b0 = __float_as_uint(y0);
+    b1 = __float_as_uint(y1);
+    b2 = __float_as_uint(y2);
+}
+
+__global__ void quantize_kernel(const float *__restrict__ f32, const unsigned *__restrict__ rowmax, long k, long kp,
+                                long nrows, int8_t *__restrict__ d0, int8_t *__restrict__ d1, int8_t *__restrict__ d2,
+                                int *__restrict__ expo)
+{
+    const long row = blockIdx.y;
+    const float mx = __uint_as_float(rowmax[row]);
+    const int E = mx > 0.f ? ilogbf(mx) + 1 : 0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) expo[row] = E;
+    const float sc = ldexpf(127.f, -E);
+    for (long x4 = (long)blockIdx.x * blockDim.x + threadIdx.x; x4 * 4 < kp; x4 += (long)gridDim.x * blockDim.x) {
+        uint32_t a[4], b[4], c[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const long x = x4 * 4 + j;
+            digits254(x < k ? f32[row * kp + x] * sc : 0.f, a[j], b[j], c[j]);
+        }
+        reinterpret_cast<uint32_t *>(d0 + row * kp)[x4] =
+            __byte_perm(__byte_perm(a[0], a[1], 0x0040), __byte_perm(a[2], a[3], 0x0040), 0x5410);
+        reinterpret_cast<uint32_t *>(d1 + row * kp)[x4] =
+            __byte_perm(__byte_perm(b[0], b[1], 0x0040), __byte_perm(b[2], b[3], 0x0040), 0x5410);
+        reinterpret_cast<uint32_t *>(d2 + row * kp)[x4] =
+            __byte_perm(__byte_perm(c[0], c[1], 0x0040), __byte_perm(c[2], c[3], 0x0040), 0x5410);
     }
 }
 
@@ -337,7 +388,8 @@ int build_maps(amber_cuda_ctx *c, const MapJob &job)
     do {                                                                                                        \
         cudaFuncSetAttribute(ring_rows_kernel<CC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s2);        \
         ring_rows_kernel<CC><<<g2, kThreads, s2, c->stream>>>(Y, ng, jmax, d_jc, job.nch, tw, job.kp,          \
-                                                               job.out_f64, job.out_hi, job.out_lo, job.out_f32); \
+                                                               job.out_f64, job.out_hi, job.out_lo, job.out_f32,  \
+                                                               job.rowmax);                                       \
     } while (0)
     switch (C2) {
         case 32: LAUNCH_ROWS(32); break;
@@ -348,7 +400,15 @@ int build_maps(amber_cuda_ctx *c, const MapJob &job)
         default: LAUNCH_ROWS(1); break;
     }
 #undef LAUNCH_ROWS
-    return cuda_check(c, cudaGetLastError(), "ring_rows_kernel launch");
+    if ((rc = cuda_check(c, cudaGetLastError(), "ring_rows_kernel launch"))) return rc;
+    if (job.d0) {
+        const long nrows = (long)job.nslots * job.nch;
+        dim3 gq((unsigned)std::min<long>((job.kp / 4 + 255) / 256, 64), (unsigned)nrows);
+        quantize_kernel<<<gq, 256, 0, c->stream>>>(job.out_f32, job.rowmax, ng * ng, job.kp, nrows, job.d0, job.d1,
+                                                   job.d2, job.expo);
+        rc = cuda_check(c, cudaGetLastError(), "quantize_kernel launch");
+    }
+    return rc;
 }
 
 }  // namespace amber

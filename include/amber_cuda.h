@@ -38,8 +38,11 @@ extern "C" {
 #define AMBER_ERR_NODEV (-7)    /* no usable sm_100 device: the library has no CPU fallback */
 
 /* ---- precision of the triple-product contraction ---- */
-#define AMBER_PREC_FP64 0  /* plain FP64 restatement of the reference loop (CUDA cores) */
-#define AMBER_PREC_MIXED 1 /* split-BF16×3 tcgen05/TMEM contraction, FP32 tiles, FP64 lag reduction */
+#define AMBER_PREC_FP64 0   /* plain FP64 restatement of the reference loop (CUDA cores) */
+#define AMBER_PREC_MIXED 1  /* int8 tensor cores: 3-digit fixed point, exact int32 accumulation in TMEM,
+                               FP64 recombination and compensated lag reduction (≤1e-6 of Σ|products|) */
+#define AMBER_PREC_BF16X3 2 /* split-BF16×3 on the tensor cores with FP32 accumulation in TMEM; kept for
+                               comparison: it misses 1e-6 on coherent v2 sampling-mask sums */
 
 typedef struct amber_cuda_ctx amber_cuda_ctx;
 
@@ -48,7 +51,7 @@ typedef struct amber_cuda_opts {
     int precision;         /* AMBER_PREC_FP64 or AMBER_PREC_MIXED */
     size_t hbm_budget;     /* max device bytes the context may hold; 0 = 90 % of free memory */
     void *stream;          /* optional cudaStream_t to launch on (NULL = the context's own stream) */
-    int chunk_px;          /* mixed path: pixels per FP32 accumulation chunk before the FP64 flush (0 = default) */
+    int chunk_px;          /* tensor-core paths: pixels per CTA accumulation chunk before the FP64 flush (0 = default) */
 } amber_cuda_opts;
 
 AMBER_API void amber_cuda_default_opts(amber_cuda_opts *opts);
