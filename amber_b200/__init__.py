@@ -28,7 +28,7 @@ LIB_PATH = os.path.join(HERE, "libamber_cuda.so")
 AMBER_OK = 0
 ERRORS = {-1: "bad argument", -2: "out of device memory / over budget", -3: "CUDA error", -4: "timeout",
           -5: "overflow", -6: "call order", -7: "no sm_100 device"}
-PREC = {"fp64": 0, "mixed": 1, "bf16x3": 2}
+PREC = {"fp64": 0, "mixed": 1, "bf16x3": 2, "fp64_abs": 3}
 
 # every entry point include/amber_cuda.h declares
 EXPORTS = (
@@ -36,7 +36,7 @@ EXPORTS = (
     "amber_cuda_load_grid_packed", "amber_cuda_load_grid", "amber_cuda_set_rings", "amber_cuda_get_uavg",
     "amber_cuda_set_channels", "amber_cuda_calcr", "amber_cuda_ng1", "amber_cuda_triangle_v1",
     "amber_cuda_triangle_v2", "amber_cuda_triangles", "amber_cuda_triangles_run", "amber_cuda_triangles_fetch",
-    "amber_cuda_last_run_stats", "amber_cuda_grid_vis",
+    "amber_cuda_last_run_stats", "amber_cuda_last_run_breakdown", "amber_cuda_grid_vis",
 )
 
 
@@ -92,6 +92,8 @@ def load_library():
     L.amber_cuda_triangles_run.argtypes = [_vp, ctypes.c_int, _ip, ctypes.c_int]
     L.amber_cuda_triangles_fetch.argtypes = [_vp, _dp, _i64p, _dp]
     L.amber_cuda_last_run_stats.argtypes = [_vp, _dp, _dp]
+    L.amber_cuda_last_run_breakdown.argtypes = [_vp, _dp, _dp, _dp, ctypes.POINTER(ctypes.c_long),
+                                                ctypes.POINTER(ctypes.c_long)]
     L.amber_cuda_grid_vis.argtypes = [_vp, ctypes.c_long, ctypes.c_long, ctypes.c_double, ctypes.c_double,
                                       ctypes.c_float, ctypes.c_int, ctypes.c_long, ctypes.c_long, ctypes.c_long, _fp,
                                       _fp, _dp, _dp]
@@ -240,6 +242,19 @@ class Estimator:
         p, ms = ctypes.c_double(), ctypes.c_double()
         self._check(self._L.amber_cuda_last_run_stats(self._h, ctypes.byref(p), ctypes.byref(ms)))
         return p.value, ms.value
+
+    def last_run_breakdown(self):
+        """(ms_maps, ms_contract, ms_reduce, kernel_launches, contract_launches) of the last run."""
+        a, b, c = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        n, m = ctypes.c_long(), ctypes.c_long()
+        self._check(self._L.amber_cuda_last_run_breakdown(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c),
+                                                          ctypes.byref(n), ctypes.byref(m)))
+        return a.value, b.value, c.value, n.value, m.value
+
+    def fetch_into(self, bldnu_ptr: int, numtri_ptr: int | None = None):
+        """Copy the last run's FP64 lag arrays into caller-owned (e.g. pinned) host memory."""
+        self._check(self._L.amber_cuda_triangles_fetch(self._h, ctypes.cast(bldnu_ptr, _dp), None,
+                                                       None if numtri_ptr is None else ctypes.cast(numtri_ptr, _dp)))
 
     # ---- gridding ---------------------------------------------------------
     def grid_vis(self, nn, nc, du, umax, nu_chan0, flag_key, randpar, data):

@@ -91,6 +91,24 @@ int twiddle_table(amber_cuda_ctx *c, long n, const double2 **out)
     return AMBER_OK;
 }
 
+void phase_begin(amber_cuda_ctx *c, int phase)
+{
+    if (c->phase_used == c->phase_ev.size()) {
+        amber_cuda_ctx::PhaseEv e;
+        cudaEventCreate(&e.a);
+        cudaEventCreate(&e.b);
+        c->phase_ev.push_back(e);
+    }
+    c->phase_ev[c->phase_used].phase = phase;
+    cudaEventRecord(c->phase_ev[c->phase_used].a, c->stream);
+}
+
+void phase_end(amber_cuda_ctx *c)
+{
+    cudaEventRecord(c->phase_ev[c->phase_used].b, c->stream);
+    ++c->phase_used;
+}
+
 namespace {
 
 // normalize_data (amber_funcs.c:1946-1978): GV /= NTiG where NTiG > 0, then
@@ -200,7 +218,8 @@ int amber_cuda_create(const amber_cuda_opts *opts, amber_cuda_ctx **out)
     amber_cuda_opts o;
     amber_cuda_default_opts(&o);
     if (opts) o = *opts;
-    if (o.precision != AMBER_PREC_FP64 && o.precision != AMBER_PREC_MIXED && o.precision != AMBER_PREC_BF16X3)
+    if (o.precision != AMBER_PREC_FP64 && o.precision != AMBER_PREC_MIXED && o.precision != AMBER_PREC_BF16X3 &&
+        o.precision != AMBER_PREC_FP64_ABS)
         return AMBER_ERR_ARG;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= o.device) {
@@ -212,7 +231,8 @@ int amber_cuda_create(const amber_cuda_opts *opts, amber_cuda_ctx **out)
     if (cudaSetDevice(o.device) != cudaSuccess) return AMBER_ERR_NODEV;
     amber_cuda_ctx *c = new amber_cuda_ctx();
     c->device = o.device;
-    c->precision = o.precision;
+    c->precision = o.precision == AMBER_PREC_FP64_ABS ? AMBER_PREC_FP64 : o.precision;
+    c->fp64_abs = o.precision == AMBER_PREC_FP64_ABS;
     c->chunk_px = o.chunk_px;
     c->num_sms = prop.multiProcessorCount;
     size_t fr = 0, tot = 0;
@@ -239,6 +259,10 @@ void amber_cuda_destroy(amber_cuda_ctx *c)
                       &c->partial, &c->results, &c->ring_lohi, &c->misc, &c->mixed_scratch};
     for (DevBuf *b : bufs) release(c, *b);
     for (auto &kv : c->twiddles) release(c, kv.second);
+    for (auto &e : c->phase_ev) {
+        cudaEventDestroy(e.a);
+        cudaEventDestroy(e.b);
+    }
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     if (c->own_stream) cudaStreamDestroy(c->stream);
@@ -450,6 +474,9 @@ int amber_cuda_triangles_run(amber_cuda_ctx *c, int ntri, const int *tri, int wa
     const size_t vbytes = prec == AMBER_PREC_FP64 ? 8 : (prec == AMBER_PREC_MIXED ? 7 : 4);
     const long kalign = prec == AMBER_PREC_MIXED ? 128 : 64;
     c->last_products = 0;
+    c->phase_used = 0;
+    c->launches = 0;
+    c->contractions = 0;
     cudaEventRecord(c->ev0, c->stream);
     for (const Group &g : groups) {
         const long k = g.ng * g.ng, kp = (k + kalign - 1) / kalign * kalign;
@@ -533,7 +560,10 @@ int amber_cuda_triangles_run(amber_cuda_ctx *c, int ntri, const int *tri, int wa
                     (rc = cuda_check(c, cudaMemsetAsync(job.rowmax, 0, sizeof(unsigned) * nrows, c->stream),
                                      "row max reset")))
                     return rc;
-                if ((rc = build_maps(c, job))) return rc;
+                phase_begin(c, 0);
+                rc = build_maps(c, job);
+                phase_end(c);
+                if (rc) return rc;
             }
             for (int t : batch) {
                 const size_t s1 = ms.slot_of_ring[tri[3 * t]], s2 = ms.slot_of_ring[tri[3 * t + 1]],
@@ -573,6 +603,12 @@ int amber_cuda_triangles_run(amber_cuda_ctx *c, int ntri, const int *tri, int wa
     if ((rc = cuda_check(c, cudaEventSynchronize(c->ev1), "triangle run"))) return rc;
     if ((rc = cuda_check(c, cudaGetLastError(), "triangle run"))) return rc;
     cudaEventElapsedTime(&c->last_ms, c->ev0, c->ev1);
+    for (int i = 0; i < 3; ++i) c->phase_ms[i] = 0;
+    for (size_t i = 0; i < c->phase_used; ++i) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, c->phase_ev[i].a, c->phase_ev[i].b);
+        c->phase_ms[c->phase_ev[i].phase] += ms;
+    }
     c->last_ntri = ntri;
     c->last_v2 = want_v2;
     return AMBER_OK;
@@ -616,6 +652,18 @@ int amber_cuda_last_run_stats(const amber_cuda_ctx *c, double *products, double 
     if (!c) return AMBER_ERR_ARG;
     if (products) *products = c->last_products;
     if (device_ms) *device_ms = c->last_ms;
+    return AMBER_OK;
+}
+
+int amber_cuda_last_run_breakdown(const amber_cuda_ctx *c, double *ms_maps, double *ms_contract, double *ms_reduce,
+                                  long *kernel_launches, long *contract_launches)
+{
+    if (!c) return AMBER_ERR_ARG;
+    if (ms_maps) *ms_maps = c->phase_ms[0];
+    if (ms_contract) *ms_contract = c->phase_ms[1];
+    if (ms_reduce) *ms_reduce = c->phase_ms[2];
+    if (kernel_launches) *kernel_launches = c->launches;
+    if (contract_launches) *contract_launches = c->contractions;
     return AMBER_OK;
 }
 

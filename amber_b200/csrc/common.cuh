@@ -76,6 +76,18 @@ struct amber_cuda_ctx {
     amber::DevBuf misc;
     amber::DevBuf mixed_scratch;
 
+    // per-phase device timing of the last run (CUDA events on the launch stream)
+    struct PhaseEv {
+        int phase;  // 0 maps, 1 contraction kernel, 2 lag reduction
+        cudaEvent_t a, b;
+    };
+    std::vector<PhaseEv> phase_ev;
+    size_t phase_used = 0;
+    double phase_ms[3] = {0, 0, 0};
+    long launches = 0;     // our kernels launched during the last run
+    long contractions = 0; // contraction-kernel launches during the last run
+    bool fp64_abs = false; // FP64 path sums |products| (the error scale of the mixed path)
+
     // last run
     int last_ntri = 0;
     int last_v2 = 0;
@@ -85,6 +97,10 @@ struct amber_cuda_ctx {
 };
 
 namespace amber {
+
+// Record a phase boundary on the context's stream (timing of the last run).
+void phase_begin(amber_cuda_ctx *c, int phase);
+void phase_end(amber_cuda_ctx *c);
 
 int fail(amber_cuda_ctx *c, int code, const char *fmt, ...);
 int cuda_check(amber_cuda_ctx *c, cudaError_t e, const char *what);

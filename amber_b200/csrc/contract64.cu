@@ -30,7 +30,7 @@ __global__ void __launch_bounds__(256) contract64_kernel(const double *__restric
                                                           const double *__restrict__ m3, long k, long kp,
                                                           const int *__restrict__ anchors,
                                                           const int *__restrict__ weight, int nc, int nc10, int tiles,
-                                                          long kchunk, double *__restrict__ partial)
+                                                          long kchunk, int use_abs, double *__restrict__ partial)
 {
     // rows padded by 2 doubles: the transposed stores hit 8 distinct bank pairs
     __shared__ __align__(16) double As[2][KB][TT + 2];
@@ -84,6 +84,10 @@ __global__ void __launch_bounds__(256) contract64_kernel(const double *__restric
                     double s1 = c1[x];
                     if (pr >= 0) va = s1 * m2[(long)pr * kp + x];
                     if (pc >= 0) vb = m3[(long)pc * kp + x];
+                    if (use_abs) {
+                        va = fabs(va);
+                        vb = fabs(vb);
+                    }
                 }
                 As[buf][xx][r] = va;
                 Bs[buf][xx][r] = vb;
@@ -179,7 +183,10 @@ __global__ void sum_fixed(const double *__restrict__ part, int n, double *__rest
 
 int lag_reduce(amber_cuda_ctx *c, const double *partial, long nunits, long ncsize, double *lag)
 {
+    phase_begin(c, 2);
     lag_reduce_kernel<<<(unsigned)((ncsize + 255) / 256), 256, 0, c->stream>>>(partial, nunits, ncsize, lag);
+    phase_end(c);
+    c->launches += 1;
     return cuda_check(c, cudaGetLastError(), "lag_reduce_kernel launch");
 }
 
@@ -202,9 +209,13 @@ int contract_fp64(amber_cuda_ctx *c, const double *m1, const double *m2, const d
     int rc = ensure(c, c->partial, pbytes, "partial lag tiles");
     if (rc) return rc;
     dim3 grid((unsigned)(tiles * tiles), (unsigned)nA, (unsigned)KS);
+    phase_begin(c, 1);
     contract64_kernel<<<grid, 256, 0, c->stream>>>(m1, m2, m3, k, kp, (const int *)c->d_anchors.p,
                                                    (const int *)c->d_weight.p, (int)c->nc, nc10, tiles, kchunk,
-                                                   (double *)c->partial.p);
+                                                   c->fp64_abs ? 1 : 0, (double *)c->partial.p);
+    phase_end(c);
+    c->launches += 1;
+    c->contractions += 1;
     if ((rc = cuda_check(c, cudaGetLastError(), "contract64_kernel launch"))) return rc;
     return lag_reduce(c, (const double *)c->partial.p, (long)nA * KS, ncsize, lag_out);
 }

@@ -351,7 +351,11 @@ int launch(amber_cuda_ctx *c, const CUtensorMap &t0, const CUtensorMap &t1, cons
 {
     const size_t sm = smem_bytes<BN>();
     cudaFuncSetAttribute(contract_i8_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    phase_begin(c, 1);
     contract_i8_kernel<BN><<<(unsigned)items, NTHREADS, sm, c->stream>>>(t0, t1, t2, prm);
+    phase_end(c);
+    c->launches += 1;
+    c->contractions += 1;
     return cuda_check(c, cudaGetLastError(), "contract_i8_kernel launch");
 }
 

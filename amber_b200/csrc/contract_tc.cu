@@ -336,7 +336,11 @@ int launch(amber_cuda_ctx *c, const CUtensorMap &th, const CUtensorMap &tl, cons
 {
     const size_t sm = smem_bytes<P, BN>();
     cudaFuncSetAttribute(contract_tc_kernel<P, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    phase_begin(c, 1);
     contract_tc_kernel<P, BN><<<(unsigned)items, NTHREADS, sm, c->stream>>>(th, tl, prm);
+    phase_end(c);
+    c->launches += 1;
+    c->contractions += 1;
     return cuda_check(c, cudaGetLastError(), "contract_tc_kernel launch");
 }
 

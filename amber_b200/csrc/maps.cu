@@ -376,6 +376,7 @@ int build_maps(amber_cuda_ctx *c, const MapJob &job)
         default: LAUNCH_COLS(1); break;
     }
 #undef LAUNCH_COLS
+    c->launches += 1;
     if ((rc = cuda_check(c, cudaGetLastError(), "ring_cols_kernel launch"))) return rc;
 
     // pass 2
@@ -400,12 +401,14 @@ int build_maps(amber_cuda_ctx *c, const MapJob &job)
         default: LAUNCH_ROWS(1); break;
     }
 #undef LAUNCH_ROWS
+    c->launches += 1;
     if ((rc = cuda_check(c, cudaGetLastError(), "ring_rows_kernel launch"))) return rc;
     if (job.d0) {
         const long nrows = (long)job.nslots * job.nch;
         dim3 gq((unsigned)std::min<long>((job.kp / 4 + 255) / 256, 64), (unsigned)nrows);
         quantize_kernel<<<gq, 256, 0, c->stream>>>(job.out_f32, job.rowmax, ng * ng, job.kp, nrows, job.d0, job.d1,
                                                    job.d2, job.expo);
+        c->launches += 1;
         rc = cuda_check(c, cudaGetLastError(), "quantize_kernel launch");
     }
     return rc;

@@ -1,0 +1,355 @@
+"""Benchmark of the AMBER estimator hot path on B200.
+
+Workload (one "step"): the single-realisation case — a 256² uv grid, 128
+channels (channels 0-1 and 30-31 of every 32-channel block flagged), 16
+log-spaced annular bins from 2 to 120 cells, all lag pairs |Δν| < 64
+(nc10 = 63), v2 output — pushed through the whole estimator: calCR, then for
+all 218 closed triangles the ring maps and the triple-product lag
+accumulation of both the visibility maps (bldnu) and the sampling-mask maps
+(numdnu).  Inputs are seeded synthetic data of that shape (there is no
+public dataset for this path).
+
+Metric: lag-triple products per second, one product being one term
+D_r1(x,p1)·D_r2(x,p2)·D_r3(x,p3) of the reference's loop (4_fbe/amber.c:261-263);
+per triangle total_vcp·Ng1², counted for the D and the I (mask) sums.
+
+* value — device time of the run with the grid already resident in HBM;
+* e2e   — the same through the C ABI from pinned host buffers: grid upload and
+  normalisation, rings, channels, calCR, the run, and the copy of every lag
+  array back to the host, all inside the timed region;
+* fp64_plain — the plain FP64 GPU path on the same GPU over a bounded sample;
+* roofline — the contraction kernel, algorithmic flops (2 per product) per
+  launch over its CUDA-event time, against the measured bf16 dense peak;
+* cpu_baseline — the reference's own OpenMP loop (oracle/_ref/ref_amber_fast,
+  its sources built unchanged) on the host cores over a bounded sample.
+
+`--impl reference` times that same reference build as the reference arm.
+Multi-GPU: one process per GPU (torchrun), each rank runs its own realisation
+(seed 1 + rank): weak scaling, no collective on the data path; timing is the
+max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "lag-triple products/s vs plain FP64 on same GPU @<=1e-6 rel err; p50/p99 latency"
+UNIT = "lag-triple products/s"
+WORKLOAD = dict(workload="single realisation: 256^2 grid, 128 channels (4 of every 32 flagged), "
+                         "16 log bins 2-120 cells, nc10=63, v2 (D and mask sums), all 218 closed triangles",
+                grid=256, channels=128, bins=16, nc10=63, du=0.5, version=2)
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return p, "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        if not shutil.which("nvidia-smi"):
+            return
+        fd, self.path = tempfile.mkstemp(prefix="clocks_", suffix=".csv")
+        os.close(fd)
+        self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                      "-i", str(self.index), "-lms", "200"], stdout=open(self.path, "w"),
+                                     stderr=subprocess.DEVNULL)
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        loaded = [s for s in sm if mx and s > 0.3 * max(mx)] or sm
+        return {"sm_mhz": float(np.median(loaded)) if loaded else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_reference_sample(real, nthreads=None, rp_pick=None, version=1, fast=True):
+    """Time the reference's own accumulation loop (ref_amber_fast) on one triangle."""
+    import oracle  # the reference build and its driver live in oracle/
+    from amber_b200 import formats
+    wd = tempfile.mkdtemp(prefix="amber_ref_")
+    try:
+        nthreads = nthreads or os.cpu_count() or 1
+        if rp_pick is None:
+            # a mid-size triangle: the first one whose largest ring is r1 = 10 (Ng1 = 218)
+            tri = oracle.triangles(real.ulow, real.uhigh)
+            rp_pick = int(np.nonzero(tri[:, 0] == 10)[0][0])
+        st, _ = oracle.run_ref_amber(real, wd, version=version, fp64=False, fast=fast, rp_begin=rp_pick,
+                                     rp_end=rp_pick + 1, nthreads=nthreads)
+        return st, rp_pick
+    finally:
+        shutil.rmtree(wd, ignore_errors=True)
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    import oracle
+    from amber_b200 import synth
+    if not oracle.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "reference build oracle/_ref missing (make -C oracle ref)"}))
+        return 0
+    real = synth.config2()
+    rates, times = [], []
+    st = None
+    for i in range(args.warmup + args.steps):
+        st, rp = cpu_reference_sample(real)
+        rate = st["products"] / st["accum_s"]
+        if i >= args.warmup:
+            rates.append(rate)
+            times.append(st["accum_s"])
+    value = float(np.median(rates))
+    sample = (f"triangle rp={rp} of the workload (Ng1=218, total_vcp={st['total_vcp']}), v1 accumulation loop "
+              f"timed like amber.c:230,285; maps excluded")
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * float(np.median(times)),
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+           "config": WORKLOAD,
+           "cpu_baseline": {"value": value, "unit": UNIT, "cores": st["threads"], "kind": "reference",
+                            "sample": sample},
+           "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="amber_b200", choices=["amber_b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    import torch
+    import torch.distributed as dist
+    import amber_b200
+    from amber_b200 import build, synth
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    build.build()
+
+    real = synth.config2(seed=1 + rank)
+    stream = torch.cuda.current_stream(dev)
+    est = amber_b200.Estimator(device=local, precision="mixed", stream=stream.cuda_stream)
+    est.load_grid(real.gv, real.counts, real.du, real.flag_key)
+    est.set_rings(real.ulow, real.uhigh)
+    est.set_channels(real.nc10, real.uf_chans)
+    rdata = est.calcr()
+    tri = rdata[:, :3].astype(np.int32)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # 256 MB > 126 MB L2
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        return float(t.item())
+
+    # ---- device-resident throughput (value) ----
+    for _ in range(args.warmup):
+        flush.zero_()
+        est.run(tri, want_v2=True)
+    clocks = Clocks(local)
+    clocks.start()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    products = 0.0
+    contract_ms = maps_ms = reduce_ms = 0.0
+    launches = contracts = 0
+    step_ms = []
+    for _ in range(args.steps):
+        flush.zero_()
+        est.run(tri, want_v2=True)
+        p, ms = est.last_run_stats()
+        a, b, c, n, m = est.last_run_breakdown()
+        products += p
+        step_ms.append(ms)
+        maps_ms += a
+        contract_ms += b
+        reduce_ms += c
+        launches += n + 1  # + the L2 flush kernel
+        contracts += m
+    e1.record(stream)
+    barrier()
+    clk = clocks.stop()
+    total_ms = max_over_ranks(e0.elapsed_time(e1))
+    all_products = sum_over_ranks(products)
+    value = all_products / (total_ms * 1e-3)
+
+    # ---- end to end through the C ABI from pinned host buffers (e2e) ----
+    ri_host = torch.from_numpy(np.ascontiguousarray(real.gv).view(np.float64)).pin_memory()
+    nt_host = torch.from_numpy(np.ascontiguousarray(real.counts)).pin_memory()
+    nclen = real.nclen
+    out_bl = torch.empty((len(tri), nclen, nclen), dtype=torch.float64).pin_memory()
+    out_nt = torch.empty((len(tri), nclen, nclen), dtype=torch.float64).pin_memory()
+    h2d = ri_host.numel() * 8 + nt_host.numel() * 8
+    d2h = out_bl.numel() * 8 + out_nt.numel() * 8 + rdata.size * 8
+
+    def e2e_step():
+        est.load_grid_raw(ri_host.data_ptr(), nt_host.data_ptr(), real.nn, real.nc, real.du, real.flag_key)
+        est.set_rings(real.ulow, real.uhigh)
+        est.set_channels(real.nc10, real.uf_chans)
+        rd = est.calcr()
+        est.run(rd[:, :3].astype(np.int32), want_v2=True)
+        est.fetch_into(out_bl.data_ptr(), out_nt.data_ptr())
+        return est.last_run_stats()[0]
+
+    for _ in range(max(1, args.warmup - 1)):
+        e2e_step()
+    barrier()
+    lat = []
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    e2e_products = 0.0
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        e2e_products += e2e_step()
+        lat.append(time.perf_counter() - t0)
+    f1.record(stream)
+    barrier()
+    e2e_ms = max_over_ranks(f0.elapsed_time(f1))
+    e2e_value = sum_over_ranks(e2e_products) / (e2e_ms * 1e-3)
+
+    # ---- plain FP64 GPU path and the mixed path's error on a bounded sample ----
+    fp64 = None
+    if rank == 0 and not args.no_fp64:
+        sample = tri[-3:]  # the three triangles with the largest map (r1 = 15, Ng1 = 740)
+        est.run(sample, want_v2=True)
+        mixed_bl, _, mixed_nt = est.fetch(want_v2=True)
+        p_mixed, ms_mixed = est.last_run_stats()
+        res = {}
+        for prec in ("fp64", "fp64_abs"):
+            with amber_b200.Estimator(device=local, precision=prec, stream=stream.cuda_stream) as e64:
+                e64.load_grid(real.gv, real.counts, real.du, real.flag_key)
+                e64.set_rings(real.ulow, real.uhigh)
+                e64.set_channels(real.nc10, real.uf_chans)
+                e64.run(sample, want_v2=True)
+                res[prec] = (e64.fetch(want_v2=True), e64.last_run_stats())
+        (bl64, _, nt64), (p64, ms64) = res["fp64"]
+        (ab_bl, _, ab_nt), _ = res["fp64_abs"]
+        err = max(float((np.abs(mixed_bl - bl64) / (ab_bl + 1e-300)).max()),
+                  float((np.abs(mixed_nt - nt64) / (ab_nt + 1e-300)).max()))
+        fp64 = {"value": p64 / (ms64 * 1e-3), "unit": UNIT,
+                "sample": "the 3 triangles with r1=15 (Ng1=740), v2, same GPU",
+                "mixed_same_sample": p_mixed / (ms_mixed * 1e-3), "speedup": (p64 / ms64) / (p_mixed / ms_mixed),
+                "max_rel_err_vs_fp64": err, "err_scale": "sum of |products| per lag cell"}
+        fp64["speedup"] = fp64["mixed_same_sample"] / fp64["value"]
+
+    # ---- CPU baseline: the reference's own loop on the host cores ----
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        try:
+            import oracle
+            if oracle.ref_available():
+                st, rp = cpu_reference_sample(real)
+                cpu = {"value": st["products"] / st["accum_s"], "unit": UNIT, "cores": st["threads"],
+                       "kind": "reference",
+                       "sample": f"one triangle (rp={rp}, Ng1=218) of this workload, v1 accumulation loop of the "
+                                 f"reference's own sources (oracle/_ref/ref_amber_fast), {st['accum_s']:.1f} s"}
+        except Exception as ex:  # reported, not fatal
+            cpu = {"value": None, "unit": UNIT, "error": str(ex)[:200]}
+
+    pk, pk_kind = peaks()
+    # algorithmic flops of one contraction launch = 2 per product; products per launch = p/(launches)
+    per_launch_products = products / max(contracts, 1)
+    avg_launch_ms = contract_ms / max(contracts, 1)
+    achieved = 2.0 * per_launch_products / (avg_launch_ms * 1e-3) / 1e12
+    peak = pk.get("bf16_tflops_sustained", pk.get("bf16_tflops"))
+    roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+            "traffic": None, "kernel": "contract_i8_kernel",
+            "peak_kind": f"{pk_kind} bf16 dense, sustained (int8 MMA nominal rate is 2x this)",
+            "per_launch_products": per_launch_products, "avg_launch_ms": avg_launch_ms,
+            "share_of_step": contract_ms / max(sum(step_ms), 1e-9),
+            "phase_ms_per_step": {"maps": maps_ms / args.steps, "contract": contract_ms / args.steps,
+                                  "lag_reduce": reduce_ms / args.steps}}
+    lat_ms = sorted(1e3 * x for x in lat)
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "int8 tensor-core digits, int32 accumulate, fp64 reduce",
+           "data": "synthetic (seeded Gaussian field, Poisson sampling, per-rank seed)",
+           "config": dict(WORKLOAD, parallelism=f"replicas x{world}", l2="256 MB flush between steps; working set "
+                                                                          "(maps) > L2"),
+           "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                   "p50_ms": float(np.percentile(lat_ms, 50)), "p99_ms": float(np.percentile(lat_ms, 99))},
+           "fp64_plain": fp64, "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
+           "gpu_launches": int(launches), "products_per_step": products / args.steps}
+    if rank == 0:
+        print(json.dumps(out))
+    est.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -43,6 +43,8 @@ extern "C" {
                                FP64 recombination and compensated lag reduction (≤1e-6 of Σ|products|) */
 #define AMBER_PREC_BF16X3 2 /* split-BF16×3 on the tensor cores with FP32 accumulation in TMEM; kept for
                                comparison: it misses 1e-6 on coherent v2 sampling-mask sums */
+#define AMBER_PREC_FP64_ABS 3 /* the FP64 path summing |products|: the per-lag-cell scale against which
+                                 the mixed path's error is measured (no reference counterpart) */
 
 typedef struct amber_cuda_ctx amber_cuda_ctx;
 
@@ -123,6 +125,12 @@ AMBER_API int amber_cuda_triangles_fetch(amber_cuda_ctx *ctx, double *bldnu, int
 /* Lag-triple products of the last run (Σ over triangles of total_vcp·Ng1²,
  * the reference's own per-triangle work) and its device time in ms. */
 AMBER_API int amber_cuda_last_run_stats(const amber_cuda_ctx *ctx, double *products, double *device_ms);
+/* Device time of the last run split into map building, the contraction
+ * kernel and the lag reduction (CUDA events on the launch stream), and how
+ * many of the library's kernels it launched.  No reference counterpart: the
+ * reference times only the whole loop (amber.c:230,285). */
+AMBER_API int amber_cuda_last_run_breakdown(const amber_cuda_ctx *ctx, double *ms_maps, double *ms_contract,
+                                            double *ms_reduce, long *kernel_launches, long *contract_launches);
 
 /* ---- gridding: replaces group_loop_gridding / _without_flag
  * (3_vcg/tgefuncs.c:377-505, 511-621).  randpar[g·npar + {0,1}] = u/ν0, v/ν0
