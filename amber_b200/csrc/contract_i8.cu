@@ -31,8 +31,11 @@
 // [anchor][chunk][lag2][lag3]; lag_reduce then sums it per lag cell with a
 // compensated FP64 accumulator in a fixed order (deterministic).
 //
-// Warp roles (320 threads): warps 0-7 form A and later read the accumulators
-// out, warp 8 issues TMA, warp 9 owns TMEM and issues the MMAs from one lane.
+// Warp roles (608 threads): warps 0-15 form A from fp32 D1/D2 tiles that warp
+// 17 stages in shared memory by TMA (3-deep ring, 128B-swizzled so the row
+// reads are conflict-free), and later read the accumulators out; warp 16
+// streams the D3 digit tiles by TMA; warp 18 owns TMEM and issues the MMAs
+// from one lane.
 // Every mbarrier wait is bounded; on expiry the CTA raises an error flag the
 // host turns into AMBER_ERR_TIMEOUT, drains its own copies and MMAs, frees TMEM.
 #include <algorithm>
@@ -49,23 +52,27 @@ using namespace tc;
 
 constexpr int BM = 128;        // p2 rows per tile = TMEM lanes
 constexpr int KB_B = 128;      // pixels per B stage: one 128-byte swizzle row of int8
-constexpr int KB_A = 64;       // pixels per A stage in TMEM
-constexpr int NSA = 2;         // A stages
+constexpr int KB_A = 64;       // pixels per A stage in TMEM (two 32-pixel fp32 input boxes)
+constexpr int NSA = 2;         // A stages in TMEM
+constexpr int NSI = 3;         // fp32 input stages in shared memory
 constexpr int NACC = 4;        // int32 accumulators, one per digit class i+j = 0..3
 constexpr int A_COL0 = 384;    // TMEM columns [384, 480) hold the A stages
 constexpr int A_STAGE_COLS = 48;  // 3 digits × 16 columns (64 int8 per lane per digit)
-constexpr int NWARP_A = 8;
-constexpr int WARP_TMA = 8;
-constexpr int WARP_MMA = 9;
-constexpr int NTHREADS = 320;
+constexpr int NWARP_A = 16;    // A-forming / epilogue warps: 4 warpgroups, 16 pixels each per A stage
+constexpr int WARP_TMA_B = 16;
+constexpr int WARP_TMA_A = 17;
+constexpr int WARP_MMA = 18;
+constexpr int NTHREADS = 19 * 32;
 constexpr int TMEM_COLS = 512;
+constexpr int IN_D2 = BM * KB_A * 4;  // bytes of one D2 input stage (two swizzled 32-pixel boxes)
+constexpr int IN_D1 = KB_A * 4;       // bytes of the D1 row of one input stage
+constexpr int IN_STAGE = IN_D2 + 1024;  // D1 row padded to keep 1024-byte alignment
 
 struct ParamsI8 {
-    const float *f1, *f2;     // D1, D2 FP32 planes [nc][kp]
     const int *e1, *e2, *e3;  // row exponents [nc]
     long k, kp;
     int nc, nc10, nclen;
-    int mt_count, nt_count, nchunk;
+    int mt_count, nt_count, nchunk, nanchors;
     long chunk;  // pixels per chunk (multiple of KB_B)
     const int *anchors;
     const int *weight;
@@ -94,47 +101,71 @@ __device__ __forceinline__ uint32_t pack_low_bytes(uint32_t a, uint32_t b, uint3
     return __byte_perm(__byte_perm(a, b, 0x0040), __byte_perm(c, d, 0x0040), 0x5410);
 }
 
+__device__ __forceinline__ void tmem_st4(uint32_t taddr, uint32_t a, uint32_t b, uint32_t c, uint32_t d)
+{
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1, %2, %3, %4};" ::"r"(taddr), "r"(a), "r"(b),
+                 "r"(c), "r"(d)
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&v)[8])
+{
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+                 : "r"(taddr)
+                 : "memory");
+}
+
 template <int BN>
 __global__ void __launch_bounds__(NTHREADS, 1)
     contract_i8_kernel(const __grid_constant__ CUtensorMap tm0, const __grid_constant__ CUtensorMap tm1,
-                       const __grid_constant__ CUtensorMap tm2, const ParamsI8 prm)
+                       const __grid_constant__ CUtensorMap tm2, const __grid_constant__ CUtensorMap tmd2,
+                       const __grid_constant__ CUtensorMap tmd1, const ParamsI8 prm)
 {
     constexpr int TILE = BN * KB_B;  // bytes of one digit tile
     constexpr int STAGE_B = 3 * TILE;
-    constexpr int NSB = (200 * 1024 / STAGE_B) < 4 ? (200 * 1024 / STAGE_B) : 4;
+    constexpr int NSB = ((200 * 1024 - NSI * IN_STAGE) / STAGE_B) < 4 ? ((200 * 1024 - NSI * IN_STAGE) / STAGE_B) : 4;
+    static_assert(NSB >= 2, "shared memory too small for the B stages");
     static_assert(NACC * BN <= A_COL0, "the int32 accumulators must fit below the A region");
     static_assert(A_COL0 + NSA * A_STAGE_COLS <= TMEM_COLS, "A stages must fit in TMEM");
     static_assert(BN % 32 == 0 && BN >= 32 && BN <= 96, "BN");
 
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char *smem = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-    unsigned char *b_tiles = smem;  // NSB × {d0, d1, d2}
-    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + NSB * STAGE_B);
+    unsigned char *in_tiles = smem;                        // NSI × {D2 box 0, D2 box 1, D1 row}
+    unsigned char *b_tiles = smem + NSI * IN_STAGE;        // NSB × {d0, d1, d2}
+    uint64_t *bars = reinterpret_cast<uint64_t *>(b_tiles + NSB * STAGE_B);
     uint64_t *b_full = bars, *b_empty = bars + NSB;
-    uint64_t *a_full = bars + 2 * NSB, *a_empty = bars + 2 * NSB + NSA;
-    uint64_t *acc_full = bars + 2 * NSB + 2 * NSA;
+    uint64_t *a_full = bars + 2 * NSB, *a_empty = a_full + NSA;
+    uint64_t *in_full = a_empty + NSA, *in_empty = in_full + NSI;
+    uint64_t *acc_full = in_empty + NSI;
     uint64_t *drain = acc_full + 1;
     volatile uint32_t *tmem_slot = reinterpret_cast<volatile uint32_t *>(drain + 1);
     volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
+    // Chunk-major order: the CTAs resident at one time share a pixel chunk, so
+    // that chunk of every map row stays in L2 while all anchors read it.
     long item = blockIdx.x;
-    const int chunk = (int)(item % prm.nchunk);
-    item /= prm.nchunk;
     const int nt = (int)(item % prm.nt_count);
     item /= prm.nt_count;
     const int mt = (int)(item % prm.mt_count);
-    const int aidx = (int)(item / prm.mt_count);
+    item /= prm.mt_count;
+    const int aidx = (int)(item % prm.nanchors);
+    const int chunk = (int)(item / prm.nanchors);
     const int p1 = prm.anchors[aidx];
     const long x_begin = (long)chunk * prm.chunk;
     const long x_end = min(prm.k, x_begin + prm.chunk);
     const int nb = (int)((x_end - x_begin + KB_B - 1) / KB_B);  // B stages; 2 A stages each
+    const int na = 2 * nb;
     const int bbase = p1 - prm.nc10 + nt * BN;                  // first p3 row of the B tile
+    const int rbase = p1 - prm.nc10 + mt * BM;                  // first p2 row of the A tile
 
     if (tid == 0) {
         for (int s = 0; s < NSB; ++s) { mbar_init(&b_full[s], 1); mbar_init(&b_empty[s], 1); }
         for (int s = 0; s < NSA; ++s) { mbar_init(&a_full[s], NWARP_A); mbar_init(&a_empty[s], 1); }
+        for (int s = 0; s < NSI; ++s) { mbar_init(&in_full[s], 1); mbar_init(&in_empty[s], NWARP_A); }
         mbar_init(acc_full, 1);
         mbar_init(drain, 1);
         *abort_flag = 0;
@@ -151,7 +182,8 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     fence_after();
     const uint32_t tmem = *tmem_slot;
 
-    if (warp == WARP_TMA) {
+    if (warp == WARP_TMA_B) {
+        // B operand: the D3 digit planes, 128 pixels × BN rows per stage
         if (lane == 0) {
             int issued = 0;
             for (int it = 0; it < nb; ++it) {
@@ -165,13 +197,31 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                 tma_load_2d(t0 + 2 * TILE, &tm2, &b_full[s], x, bbase);
                 ++issued;
             }
-            if (*abort_flag) {
-                for (int it = max(0, issued - NSB); it < issued; ++it) {
-                    const int s = it % NSB;
-                    for (long long i = 0; i < WAIT_LIMIT && !mbar_try_wait(&b_full[s], (it / NSB) & 1); ++i)
+            if (*abort_flag)
+                for (int it = max(0, issued - NSB); it < issued; ++it)
+                    for (long long i = 0; i < WAIT_LIMIT && !mbar_try_wait(&b_full[it % NSB], (it / NSB) & 1); ++i)
                         __nanosleep(100);
-                }
+        }
+    } else if (warp == WARP_TMA_A) {
+        // A inputs: 64 pixels of the 128 D2 rows (two swizzled 32-pixel boxes) and of the D1 row.
+        // Pixels past the end of the map come back as zeros, rows outside [0, nc) too.
+        if (lane == 0) {
+            int issued = 0;
+            for (int ia = 0; ia < na; ++ia) {
+                const int s = ia % NSI;
+                if (!mbar_wait(&in_empty[s], ((ia / NSI) & 1) ^ 1, abort_flag, prm.err, 6)) break;
+                unsigned char *t = in_tiles + s * IN_STAGE;
+                mbar_expect_tx(&in_full[s], IN_D2 + IN_D1);
+                const int x = (int)(x_begin + (long)ia * KB_A);
+                tma_load_2d(t, &tmd2, &in_full[s], x, rbase);
+                tma_load_2d(t + IN_D2 / 2, &tmd2, &in_full[s], x + 32, rbase);
+                tma_load_2d(t + IN_D2, &tmd1, &in_full[s], x, p1);
+                ++issued;
             }
+            if (*abort_flag)
+                for (int ia = max(0, issued - NSI); ia < issued; ++ia)
+                    for (long long i = 0; i < WAIT_LIMIT && !mbar_try_wait(&in_full[ia % NSI], (ia / NSI) & 1); ++i)
+                        __nanosleep(100);
         }
     } else if (warp == WARP_MMA) {
         if (lane == 0) {
@@ -218,75 +268,73 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             }
         }
     } else {
-        // ---- A formation: warps 0-7; warpgroup wg covers pixels [32·wg, 32·wg + 32) of each A stage ----
-        const int wg = warp >> 2;
+        // ---- A formation: warps 0-15; warpgroup g covers pixels [16g, 16g + 16) of each A stage ----
+        const int g = warp >> 2;
         const int m = ((warp & 3) << 5) + lane;
         const uint32_t lane_field = (uint32_t)((warp & 3) << 5) << 16;
         const int d2 = mt * BM + m;
-        const int p2 = p1 - prm.nc10 + d2;
+        const int p2 = rbase + m;
         const bool row_ok = d2 < prm.nclen && p2 >= 0 && p2 < prm.nc && prm.weight[p2] > 0;
         const int E1 = prm.e1[p1];
         const int E2 = row_ok ? prm.e2[p2] : 0;
-        const float scale = ldexpf(127.f, -(E1 + E2));  // A·127·2^−(E1+E2) ∈ [−127, 127]
-        const float *r1 = prm.f1 + (long)p1 * prm.kp;
-        const float *r2 = prm.f2 + (long)(row_ok ? p2 : 0) * prm.kp;
+        const float scale = row_ok ? ldexpf(127.f, -(E1 + E2)) : 0.f;  // A·127·2^−(E1+E2) ∈ [−127, 127]
+        // this thread's 16 pixels: 16-byte chunks j0..j0+3 of one 32-pixel box, 128B-swizzled by row
+        const int box = g >> 1, j0 = (g & 1) * 4;
+        const int px0 = g * 16;
         bool ok = true;
-        const int na = 2 * nb;
         for (int ia = 0; ia < na; ++ia) {
-            const int sa = ia % NSA;
+            const int si = ia % NSI, sa = ia % NSA;
+            if (!mbar_wait_warp(&in_full[si], (ia / NSI) & 1, abort_flag, prm.err, 7)) { ok = false; break; }
+            const unsigned char *t = in_tiles + si * IN_STAGE;
+            const float *rowp = reinterpret_cast<const float *>(t + box * (IN_D2 / 2) + m * 128);
+            const float *d1p = reinterpret_cast<const float *>(t + IN_D2) + px0;
+            uint32_t w[3][4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const float4 v = *reinterpret_cast<const float4 *>(rowp + (((j0 + q) ^ (m & 7)) << 2));
+                const float4 u = *reinterpret_cast<const float4 *>(d1p + 4 * q);
+                uint32_t a[4], b[4], c[4];
+                digits254(u.x * v.x * scale, a[0], b[0], c[0]);
+                digits254(u.y * v.y * scale, a[1], b[1], c[1]);
+                digits254(u.z * v.z * scale, a[2], b[2], c[2]);
+                digits254(u.w * v.w * scale, a[3], b[3], c[3]);
+                w[0][q] = pack_low_bytes(a[0], a[1], a[2], a[3]);
+                w[1][q] = pack_low_bytes(b[0], b[1], b[2], b[3]);
+                w[2][q] = pack_low_bytes(c[0], c[1], c[2], c[3]);
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&in_empty[si]);
             if (!mbar_wait_warp(&a_empty[sa], ((ia / NSA) & 1) ^ 1, abort_flag, prm.err, 4)) { ok = false; break; }
             fence_after();
-            const long x = x_begin + (long)ia * KB_A + wg * 32;
-            uint32_t w0[8], w1[8], w2[8];
-            if (row_ok && x < x_end) {
-#pragma unroll
-                for (int q = 0; q < 8; ++q) {
-                    const float4 u = __ldg(reinterpret_cast<const float4 *>(r1 + x) + q);
-                    const float4 v = __ldg(reinterpret_cast<const float4 *>(r2 + x) + q);
-                    float t[4] = {u.x * v.x * scale, u.y * v.y * scale, u.z * v.z * scale, u.w * v.w * scale};
-                    uint32_t a[4], b[4], cc[4];
-#pragma unroll
-                    for (int j = 0; j < 4; ++j) {
-                        if (x + 4 * q + j >= x_end) t[j] = 0.f;
-                        digits254(t[j], a[j], b[j], cc[j]);
-                    }
-                    w0[q] = pack_low_bytes(a[0], a[1], a[2], a[3]);
-                    w1[q] = pack_low_bytes(b[0], b[1], b[2], b[3]);
-                    w2[q] = pack_low_bytes(cc[0], cc[1], cc[2], cc[3]);
-                }
-            } else {
-#pragma unroll
-                for (int q = 0; q < 8; ++q) { w0[q] = 0u; w1[q] = 0u; w2[q] = 0u; }
-            }
-            const uint32_t col = tmem + lane_field + A_COL0 + sa * A_STAGE_COLS + wg * 8;
-            tmem_st8(col, w0);
-            tmem_st8(col + 16, w1);
-            tmem_st8(col + 32, w2);
+            const uint32_t col = tmem + lane_field + A_COL0 + sa * A_STAGE_COLS + g * 4;
+            tmem_st4(col, w[0][0], w[0][1], w[0][2], w[0][3]);
+            tmem_st4(col + 16, w[1][0], w[1][1], w[1][2], w[1][3]);
+            tmem_st4(col + 32, w[2][0], w[2][1], w[2][2], w[2][3]);
             asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
             fence_before();
             __syncwarp();
             if (lane == 0) mbar_arrive(&a_full[sa]);
         }
 
-        // ---- epilogue: int32 digit accumulators → FP64 partial tile ----
+        // ---- epilogue: int32 digit accumulators → FP64 partial tile; warpgroup g reads BN/4 columns ----
         if (ok && mbar_wait_warp(acc_full, 0, abort_flag, prm.err, 5)) {
             fence_after();
             const double wr = row_ok ? (double)prm.weight[p1] * (double)prm.weight[p2] : 0.0;
             double *dst = nullptr;
             if (d2 < prm.nclen)
                 dst = prm.partial + ((long)aidx * prm.nchunk + chunk) * prm.nclen * prm.nclen + (long)d2 * prm.nclen;
-            const int c_begin = wg * (BN / 2), c_end = c_begin + BN / 2;
-            for (int c0 = c_begin; c0 < c_end; c0 += 16) {
-                uint32_t v0[16], v1[16], v2[16], v3[16];
-                tmem_ld16(tmem + lane_field + c0, v0);
-                tmem_ld16(tmem + lane_field + BN + c0, v1);
-                tmem_ld16(tmem + lane_field + 2 * BN + c0, v2);
-                tmem_ld16(tmem + lane_field + 3 * BN + c0, v3);
+            const int c_begin = g * (BN / 4), c_end = c_begin + BN / 4;
+            const double i254 = 1.0 / 254.0, i254_2 = i254 * i254, i254_3 = i254_2 * i254;
+            for (int c0 = c_begin; c0 < c_end; c0 += 8) {
+                uint32_t v0[8], v1[8], v2[8], v3[8];
+                tmem_ld8(tmem + lane_field + c0, v0);
+                tmem_ld8(tmem + lane_field + BN + c0, v1);
+                tmem_ld8(tmem + lane_field + 2 * BN + c0, v2);
+                tmem_ld8(tmem + lane_field + 3 * BN + c0, v3);
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
                 if (dst) {
-                    const double i254 = 1.0 / 254.0, i254_2 = i254 * i254, i254_3 = i254_2 * i254;
 #pragma unroll
-                    for (int j = 0; j < 16; ++j) {
+                    for (int j = 0; j < 8; ++j) {
                         const int n = c0 + j;
                         const int d3 = nt * BN + n;
                         if (d3 >= prm.nclen) continue;
@@ -316,15 +364,16 @@ template <int BN>
 size_t smem_bytes()
 {
     constexpr int STAGE_B = 3 * BN * KB_B;
-    constexpr int NSB = (200 * 1024 / STAGE_B) < 4 ? (200 * 1024 / STAGE_B) : 4;
-    return 1024 + (size_t)NSB * STAGE_B + 256;
+    constexpr int NSB = ((200 * 1024 - NSI * IN_STAGE) / STAGE_B) < 4 ? ((200 * 1024 - NSI * IN_STAGE) / STAGE_B) : 4;
+    return 1024 + (size_t)NSI * IN_STAGE + (size_t)NSB * STAGE_B + 256;
 }
 
 typedef CUresult (*EncodeTiled)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
                                 const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
-int make_map_u8(amber_cuda_ctx *c, CUtensorMap *m, const int8_t *plane, long k, long kp, long rows, int box_rows)
+int encode(amber_cuda_ctx *c, CUtensorMap *m, CUtensorMapDataType dt, const void *plane, long k, long row_bytes,
+           long rows, int box_x, int box_rows, CUtensorMapSwizzle sw)
 {
     static EncodeTiled enc = nullptr;
     if (!enc) {
@@ -335,24 +384,23 @@ int make_map_u8(amber_cuda_ctx *c, CUtensorMap *m, const int8_t *plane, long k, 
         enc = (EncodeTiled)fn;
     }
     cuuint64_t dims[2] = {(cuuint64_t)k, (cuuint64_t)rows};
-    cuuint64_t strides[1] = {(cuuint64_t)kp};
-    cuuint32_t box[2] = {(cuuint32_t)KB_B, (cuuint32_t)box_rows};
+    cuuint64_t strides[1] = {(cuuint64_t)row_bytes};
+    cuuint32_t box[2] = {(cuuint32_t)box_x, (cuuint32_t)box_rows};
     cuuint32_t estr[2] = {1, 1};
-    CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, (void *)plane, dims, strides, box, estr,
-                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (r != CUDA_SUCCESS) return fail(c, AMBER_ERR_CUDA, "cuTensorMapEncodeTiled (int8) failed (%d)", (int)r);
+    CUresult r = enc(m, dt, 2, (void *)plane, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, sw,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(c, AMBER_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
     return AMBER_OK;
 }
 
 template <int BN>
 int launch(amber_cuda_ctx *c, const CUtensorMap &t0, const CUtensorMap &t1, const CUtensorMap &t2,
-           const ParamsI8 &prm, long items)
+           const CUtensorMap &td2, const CUtensorMap &td1, const ParamsI8 &prm, long items)
 {
     const size_t sm = smem_bytes<BN>();
     cudaFuncSetAttribute(contract_i8_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     phase_begin(c, 1);
-    contract_i8_kernel<BN><<<(unsigned)items, NTHREADS, sm, c->stream>>>(t0, t1, t2, prm);
+    contract_i8_kernel<BN><<<(unsigned)items, NTHREADS, sm, c->stream>>>(t0, t1, t2, td2, td1, prm);
     phase_end(c);
     c->launches += 1;
     c->contractions += 1;
@@ -388,12 +436,15 @@ int contract_i8(amber_cuda_ctx *c, const DigitMaps &m1, const DigitMaps &m2, con
     int *d_err = (int *)c->misc.p;
     if ((rc = cuda_check(c, cudaMemsetAsync(d_err, 0, sizeof(int), c->stream), "error flag"))) return rc;
 
-    CUtensorMap t0, t1, t2;
-    if ((rc = make_map_u8(c, &t0, m3.d0, k, kp, c->nc, BN))) return rc;
-    if ((rc = make_map_u8(c, &t1, m3.d1, k, kp, c->nc, BN))) return rc;
-    if ((rc = make_map_u8(c, &t2, m3.d2, k, kp, c->nc, BN))) return rc;
+    CUtensorMap t0, t1, t2, td2, td1;
+    const CUtensorMapDataType u8 = CU_TENSOR_MAP_DATA_TYPE_UINT8, f32 = CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+    if ((rc = encode(c, &t0, u8, m3.d0, k, kp, c->nc, KB_B, BN, CU_TENSOR_MAP_SWIZZLE_128B))) return rc;
+    if ((rc = encode(c, &t1, u8, m3.d1, k, kp, c->nc, KB_B, BN, CU_TENSOR_MAP_SWIZZLE_128B))) return rc;
+    if ((rc = encode(c, &t2, u8, m3.d2, k, kp, c->nc, KB_B, BN, CU_TENSOR_MAP_SWIZZLE_128B))) return rc;
+    if ((rc = encode(c, &td2, f32, m2.f32, k, kp * 4, c->nc, 32, BM, CU_TENSOR_MAP_SWIZZLE_128B))) return rc;
+    if ((rc = encode(c, &td1, f32, m1.f32, k, kp * 4, c->nc, KB_A, 1, CU_TENSOR_MAP_SWIZZLE_NONE))) return rc;
     ParamsI8 prm{};
-    prm.f1 = m1.f32; prm.f2 = m2.f32;
+    prm.nanchors = nA;
     prm.e1 = m1.expo; prm.e2 = m2.expo; prm.e3 = m3.expo;
     prm.k = k; prm.kp = kp;
     prm.nc = (int)c->nc; prm.nc10 = nc10; prm.nclen = nclen;
@@ -404,9 +455,9 @@ int contract_i8(amber_cuda_ctx *c, const DigitMaps &m1, const DigitMaps &m2, con
     prm.err = d_err;
     const long items = base_items * nch;
     switch (BN) {
-        case 32: rc = launch<32>(c, t0, t1, t2, prm, items); break;
-        case 64: rc = launch<64>(c, t0, t1, t2, prm, items); break;
-        case 96: rc = launch<96>(c, t0, t1, t2, prm, items); break;
+        case 32: rc = launch<32>(c, t0, t1, t2, td2, td1, prm, items); break;
+        case 64: rc = launch<64>(c, t0, t1, t2, td2, td1, prm, items); break;
+        case 96: rc = launch<96>(c, t0, t1, t2, td2, td1, prm, items); break;
         default: rc = fail(c, AMBER_ERR_ARG, "no int8 tile configuration for nclen=%d (BN=%d)", nclen, BN);
     }
     if (rc) return rc;

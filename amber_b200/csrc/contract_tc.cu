@@ -98,13 +98,14 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
     // work item → (group, m-tile, n-tile, chunk)
+    // Chunk-major order (see contract_i8.cu): resident CTAs share a pixel chunk.
     long item = blockIdx.x;
-    const int chunk = (int)(item % prm.nchunk);
-    item /= prm.nchunk;
     const int nt = (int)(item % prm.nt_count);
     item /= prm.nt_count;
     const int mt = (int)(item % prm.mt_count);
-    const int g = (int)(item / prm.mt_count);
+    item /= prm.mt_count;
+    const int g = (int)(item % prm.ngroups);
+    const int chunk = (int)(item / prm.ngroups);
     const Group grp = prm.groups[g];
     const long x_begin = (long)chunk * prm.chunk;
     const long x_end = min(prm.k, x_begin + prm.chunk);

@@ -116,9 +116,8 @@ def cpu_reference_sample(real, nthreads=None, rp_pick=None, version=1, fast=True
     try:
         nthreads = nthreads or os.cpu_count() or 1
         if rp_pick is None:
-            # a mid-size triangle: the first one whose largest ring is r1 = 10 (Ng1 = 218)
-            tri = oracle.triangles(real.ulow, real.uhigh)
-            rp_pick = int(np.nonzero(tri[:, 0] == 10)[0][0])
+            # the last triangle: largest ring r1 = 15, Ng1 = 740 — the kind of triangle that dominates the step
+            rp_pick = len(oracle.triangles(real.ulow, real.uhigh)) - 1
         st, _ = oracle.run_ref_amber(real, wd, version=version, fp64=False, fast=fast, rp_begin=rp_pick,
                                      rp_end=rp_pick + 1, nthreads=nthreads)
         return st, rp_pick
@@ -145,7 +144,7 @@ def run_reference_arm(args):
             rates.append(rate)
             times.append(st["accum_s"])
     value = float(np.median(rates))
-    sample = (f"triangle rp={rp} of the workload (Ng1=218, total_vcp={st['total_vcp']}), v1 accumulation loop "
+    sample = (f"triangle rp={rp} of the workload (Ng1=740, total_vcp={st['total_vcp']}), v1 accumulation loop "
               f"timed like amber.c:230,285; maps excluded")
     out = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * float(np.median(times)),
@@ -166,6 +165,7 @@ def main():
     ap.add_argument("--impl", default="amber_b200", choices=["amber_b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--tri-subset", default="", help="comma-separated triangle indices (profiling runs only)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -192,6 +192,8 @@ def main():
     est.set_channels(real.nc10, real.uf_chans)
     rdata = est.calcr()
     tri = rdata[:, :3].astype(np.int32)
+    if args.tri_subset:
+        tri = tri[[int(t) for t in args.tri_subset.split(",")]]
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # 256 MB > 126 MB L2
 
     def barrier():
@@ -259,7 +261,7 @@ def main():
         est.set_rings(real.ulow, real.uhigh)
         est.set_channels(real.nc10, real.uf_chans)
         rd = est.calcr()
-        est.run(rd[:, :3].astype(np.int32), want_v2=True)
+        est.run(rd[:, :3].astype(np.int32) if not args.tri_subset else tri, want_v2=True)
         est.fetch_into(out_bl.data_ptr(), out_nt.data_ptr())
         return est.last_run_stats()[0]
 
@@ -313,7 +315,7 @@ def main():
                 st, rp = cpu_reference_sample(real)
                 cpu = {"value": st["products"] / st["accum_s"], "unit": UNIT, "cores": st["threads"],
                        "kind": "reference",
-                       "sample": f"one triangle (rp={rp}, Ng1=218) of this workload, v1 accumulation loop of the "
+                       "sample": f"one triangle (rp={rp}, Ng1=740) of this workload, v1 accumulation loop of the "
                                  f"reference's own sources (oracle/_ref/ref_amber_fast), {st['accum_s']:.1f} s"}
         except Exception as ex:  # reported, not fatal
             cpu = {"value": None, "unit": UNIT, "error": str(ex)[:200]}
