@@ -96,6 +96,23 @@ __device__ __forceinline__ void digits254(float t, uint32_t &b0, uint32_t &b1, u
     b2 = __float_as_uint(y2);
 }
 
+// The same three digits for two products u·v at once, with packed FP32x2
+// arithmetic: every step is one fused op on a pair and the product u·v enters
+// the first rounding unrounded (y0 = fma(u, v, M)).  M − y = −digit exactly.
+__device__ __forceinline__ void digits254x2(float2 u, float2 v, float2 &y0, float2 &y1, float2 &y2)
+{
+    const float2 M = make_float2(12582912.0f, 12582912.0f);
+    const float2 K254 = make_float2(254.f, 254.f);
+    const float2 NEG1 = make_float2(-1.f, -1.f);
+    y0 = __ffma2_rn(u, v, M);                   // M + d0
+    const float2 nq0 = __ffma2_rn(y0, NEG1, M); // −d0
+    const float2 r0 = __ffma2_rn(u, v, nq0);    // u·v − d0
+    y1 = __ffma2_rn(r0, K254, M);               // M + d1
+    const float2 nq1 = __ffma2_rn(y1, NEG1, M); // −d1
+    const float2 s1 = __ffma2_rn(r0, K254, nq1); // 254·r0 − d1
+    y2 = __ffma2_rn(s1, K254, M);               // M + d2
+}
+
 __device__ __forceinline__ uint32_t pack_low_bytes(uint32_t a, uint32_t b, uint32_t c, uint32_t d)
 {
     return __byte_perm(__byte_perm(a, b, 0x0040), __byte_perm(c, d, 0x0040), 0x5410);
@@ -289,18 +306,20 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             const float *rowp = reinterpret_cast<const float *>(t + box * (IN_D2 / 2) + m * 128);
             const float *d1p = reinterpret_cast<const float *>(t + IN_D2) + px0;
             uint32_t w[3][4];
+            const float2 sc2 = make_float2(scale, scale);
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
                 const float4 v = *reinterpret_cast<const float4 *>(rowp + (((j0 + q) ^ (m & 7)) << 2));
                 const float4 u = *reinterpret_cast<const float4 *>(d1p + 4 * q);
-                uint32_t a[4], b[4], c[4];
-                digits254(u.x * v.x * scale, a[0], b[0], c[0]);
-                digits254(u.y * v.y * scale, a[1], b[1], c[1]);
-                digits254(u.z * v.z * scale, a[2], b[2], c[2]);
-                digits254(u.w * v.w * scale, a[3], b[3], c[3]);
-                w[0][q] = pack_low_bytes(a[0], a[1], a[2], a[3]);
-                w[1][q] = pack_low_bytes(b[0], b[1], b[2], b[3]);
-                w[2][q] = pack_low_bytes(c[0], c[1], c[2], c[3]);
+                float2 ya0, ya1, ya2, yb0, yb1, yb2;
+                digits254x2(__fmul2_rn(make_float2(u.x, u.y), sc2), make_float2(v.x, v.y), ya0, ya1, ya2);
+                digits254x2(__fmul2_rn(make_float2(u.z, u.w), sc2), make_float2(v.z, v.w), yb0, yb1, yb2);
+                w[0][q] = pack_low_bytes(__float_as_uint(ya0.x), __float_as_uint(ya0.y), __float_as_uint(yb0.x),
+                                         __float_as_uint(yb0.y));
+                w[1][q] = pack_low_bytes(__float_as_uint(ya1.x), __float_as_uint(ya1.y), __float_as_uint(yb1.x),
+                                         __float_as_uint(yb1.y));
+                w[2][q] = pack_low_bytes(__float_as_uint(ya2.x), __float_as_uint(ya2.y), __float_as_uint(yb2.x),
+                                         __float_as_uint(yb2.y));
             }
             __syncwarp();
             if (lane == 0) mbar_arrive(&in_empty[si]);
