@@ -8,7 +8,8 @@
 namespace amber {
 namespace tc {
 
-constexpr long long WAIT_LIMIT = 1LL << 24;  // × ~100 ns back-off ≈ 1.7 s
+constexpr long long WAIT_LIMIT = 1LL << 20;     // polls for drain loops (each try_wait suspends briefly)
+constexpr long long WAIT_CYCLES = 4000000000LL; // ≈ 2 s of SM clock before a pipeline wait gives up
 
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p)
@@ -34,14 +35,19 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
     return ok != 0;
 }
 
-// Bounded wait: returns false (and raises the abort flags) if the phase never completes.
+// Bounded wait: spins on try_wait (which itself suspends the thread for a
+// short hardware-defined time), gives up after WAIT_CYCLES of SM clock and
+// raises the abort flags.  No sleep in the fast path: a sleep would add its
+// wake-up latency to every producer/consumer hand-off.
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile int *abort_flag, int *err,
                                           int code)
 {
-    for (long long i = 0; i < WAIT_LIMIT; ++i) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const long long t0 = clock64();
+    while (true) {
         if (mbar_try_wait(bar, parity)) return true;
         if (*abort_flag) return false;
-        if (i > 32) __nanosleep(100);
+        if (clock64() - t0 > WAIT_CYCLES) break;
     }
     *abort_flag = 1;
     atomicExch(err, code);
