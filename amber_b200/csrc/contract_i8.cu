@@ -53,10 +53,8 @@ using namespace tc;
 constexpr int BM = 128;        // p2 rows per tile = TMEM lanes
 constexpr int KB_B = 128;      // pixels per B stage: one 128-byte swizzle row of int8
 constexpr int KB_A = 64;       // pixels per A stage in TMEM (two 32-pixel fp32 input boxes)
-constexpr int NSA = 2;         // A stages in TMEM
 constexpr int NSI = 3;         // fp32 input stages in shared memory
 constexpr int NACC = 4;        // int32 accumulators, one per digit class i+j = 0..3
-constexpr int A_COL0 = 384;    // TMEM columns [384, 480) hold the A stages
 constexpr int A_STAGE_COLS = 48;  // 3 digits × 16 columns (64 int8 per lane per digit)
 constexpr int NWARP_A = 16;    // A-forming / epilogue warps: 4 warpgroups, 16 pixels each per A stage
 constexpr int WARP_TMA_B = 16;
@@ -141,9 +139,12 @@ __global__ void __launch_bounds__(NTHREADS, 1)
 {
     constexpr int TILE = BN * KB_B;  // bytes of one digit tile
     constexpr int STAGE_B = 3 * TILE;
+    // TMEM: the four accumulators take 4·BN columns, the A stages the rest (≤ 4 stages)
+    constexpr int A_COL0 = NACC * BN;
+    constexpr int NSA = (TMEM_COLS - A_COL0) / A_STAGE_COLS < 4 ? (TMEM_COLS - A_COL0) / A_STAGE_COLS : 4;
     constexpr int NSB = ((200 * 1024 - NSI * IN_STAGE) / STAGE_B) < 4 ? ((200 * 1024 - NSI * IN_STAGE) / STAGE_B) : 4;
     static_assert(NSB >= 2, "shared memory too small for the B stages");
-    static_assert(NACC * BN <= A_COL0, "the int32 accumulators must fit below the A region");
+    static_assert(NSA >= 2, "TMEM must hold at least two A stages");
     static_assert(A_COL0 + NSA * A_STAGE_COLS <= TMEM_COLS, "A stages must fit in TMEM");
     static_assert(BN % 32 == 0 && BN >= 32 && BN <= 96, "BN");
 
@@ -246,21 +247,23 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             const uint32_t idesc = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
                                    ((uint32_t)(BM >> 4) << 24);
             const uint32_t acc0 = tmem, acc1 = tmem + BN, acc2 = tmem + 2 * BN, acc3 = tmem + 3 * BN;
+            // descriptors are linear in the start address (bits 0-13, 16-byte units): build the
+            // first one once and advance it by (byte offset >> 4)
+            const uint64_t desc0 = smem_desc_sw128(smem_u32(b_tiles));
             bool ok = true;
             uint32_t started = 0;
             for (int it = 0; it < nb && ok; ++it) {
                 const int sb = it % NSB;
                 if (!mbar_wait(&b_full[sb], (it / NSB) & 1, abort_flag, prm.err, 2)) { ok = false; break; }
-                const uint32_t tb = smem_u32(b_tiles + sb * STAGE_B);
+                const uint64_t dstage = desc0 + (uint64_t)((sb * STAGE_B) >> 4);
                 for (int h = 0; h < 2; ++h) {
                     const int ia = 2 * it + h, sa = ia % NSA;
                     if (!mbar_wait(&a_full[sa], (ia / NSA) & 1, abort_flag, prm.err, 3)) { ok = false; break; }
                     fence_after();
 #pragma unroll
                     for (int kk = 0; kk < 2; ++kk) {
-                        const uint32_t bo = (uint32_t)(2 * h + kk) * 32;
-                        const uint64_t B0 = smem_desc_sw128(tb + bo), B1 = smem_desc_sw128(tb + TILE + bo),
-                                       B2 = smem_desc_sw128(tb + 2 * TILE + bo);
+                        const uint64_t B0 = dstage + (uint64_t)((2 * h + kk) * 2), B1 = B0 + (TILE >> 4),
+                                       B2 = B0 + (2 * TILE >> 4);
                         const uint32_t a = tmem + A_COL0 + sa * A_STAGE_COLS + kk * 8;
                         const uint32_t A0 = a, A1 = a + 16, A2 = a + 32;
                         umma_ts_i8(acc0, A0, B0, idesc, started);  // i+j = 0
@@ -380,7 +383,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
 }
 
 template <int BN>
-size_t smem_bytes()
+size_t smem_bytes()  // NSB as in the kernel
 {
     constexpr int STAGE_B = 3 * BN * KB_B;
     constexpr int NSB = ((200 * 1024 - NSI * IN_STAGE) / STAGE_B) < 4 ? ((200 * 1024 - NSI * IN_STAGE) / STAGE_B) : 4;
