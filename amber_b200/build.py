@@ -55,7 +55,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if os.path.exists(drv_src) and (force or _stale(DRIVER, [drv_src, LIB])):
         cc = shutil.which("gcc") or "cc"
         subprocess.run([cc, "-O2", "-std=gnu11", "-Wall", "-I", os.path.join(ROOT, "include"), drv_src, "-o", DRIVER,
-                        "-L", HERE, "-lamber_cuda", f"-Wl,-rpath,{HERE}", "-lm"], check=True)
+                        "-L", HERE, "-lamber_cuda", "-Wl,-rpath,$ORIGIN", "-lm"], check=True)
     return LIB
 
 
