@@ -144,6 +144,32 @@ AMBER_API int amber_cuda_grid_vis(amber_cuda_ctx *ctx, long NN, long nc, double 
                         long ngroups, long npar, long nstokes, const float *randpar, const float *data,
                         double *re_im_out, double *ntig_out);
 
+/* ---- allocation-free FP64 lag contraction of one triangle.  No counterpart
+ * in the reference: it exists for callers that own every device allocation
+ * themselves — a process that reserves its HBM budget at start-up, or an
+ * application whose own caching allocator must remain the only one — and so
+ * cannot let a library call cudaMalloc.  The caller passes device pointers:
+ * the three ring-map sets m1, m2, m3 of the triangle (FP64 [nc][kp], the first
+ * k = Ng1² entries of each row used, as the reference's fill_s2d builds them)
+ * and the output lag array lag (FP64 [nclen²], nclen = 2·nc10+1, row Δ2+nc10,
+ * column Δ3+nc10).  weight is a HOST array of nc channel multiplicities
+ * (1 for every channel when the data are unflagged, the count of each channel
+ * in uf_chans otherwise).  The result equals the plain FP64 path
+ * (AMBER_PREC_FP64) of the context-based calls to FP64 rounding.
+ * Scratch: one 8 MiB file-scope device array (partial lag tiles + channel
+ * tables) that every GPU which loads the library holds until the process
+ * exits; nc ≤ 4096 and nclen² ≤ 1044480 (nc10 ≤ 510); larger sizes are
+ * rejected with AMBER_ERR_ARG.  The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress, with that device current), so
+ * make that first call before any stream capture.  Every call shares the
+ * array: calls that overlap on the GPU (different streams, or host threads)
+ * race.  Work is enqueued on `stream` (a cudaStream_t, NULL for the default
+ * stream); the caller synchronises.  err_msg (may be NULL) receives a
+ * message on failure. */
+AMBER_API int amber_cuda_contract_fp64_noalloc(const double *m1, const double *m2, const double *m3, long nc,
+                                               long k, long kp, int nc10, const int *weight, double *lag,
+                                               void *stream, char *err_msg, size_t err_len);
+
 #ifdef __cplusplus
 }
 #endif
