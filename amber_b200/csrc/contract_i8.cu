@@ -13,32 +13,50 @@
 //     D_r(x) = 2^E_r/127 · (d0 + d1/254 + d2/254²) + O(2^E_r·2^−24),
 // d0, d1, d2 ∈ [−127, 127] (quantize_kernel, maps.cu).
 // For one anchor p1 the GEMM is, as in the reference's loop,
-//     T_p1[p2, p3] = Σ_x (D1[p1,x]·D2[p2,x]) · D3[p3,x]
-// with M = p2 (128 TMEM lanes), N = p3 (BN ≤ 128), K = pixels:
-//   A = D1[p1]·D2[p2] formed in FP32 on the CUDA cores from the maps' FP32
-//       planes, scaled by 127·2^−(E1+E2) and cut into three int8 digits
-//       written straight into TMEM (tcgen05.st; the "TS" MMA form);
-//   B = the D3 digit planes, streamed by TMA into 128-byte-swizzled smem;
-//   acc_k += Σ_{i+j=k} A_i·B_jᵀ for k = 0..3 — eight kind::i8 MMAs per 32
-//       pixels into four int32 TMEM accumulators (the i+j = 4 term is below
-//       2^−31 of the leading one).  Per pixel |Σ_{i+j=k}| ≤ 3·127² < 2^15.6,
-//       so a chunk of up to 2^15 pixels cannot overflow.
-// The k = 3 class matters: dropping it leaves ~2e-6 of Σ|products| on sharply
-// peaked sampling-mask maps, keeping it gives ≤ 3e-7; four accumulators cap
-// the p3 tile at 96 columns (TMEM holds 512).
+//     T_p1[p2, p3] = Σ_x D2[p2,x] · (D1[p1,x]·D3[p3,x])
+// with M = p2 (128 TMEM lanes), N = p3 (BN ∈ {32, 64}), K = pixels:
+//   A = the D2 digit planes, staged by TMA in 64B-swizzled shared memory and
+//       moved into TMEM with tcgen05.st (the "TS" MMA form) — no per-anchor
+//       arithmetic on the 128 A rows;
+//   B = D1[p1]·D3[p3] formed in FP32 on the CUDA cores (packed FP32x2) from
+//       TMA-staged fp32 tiles, scaled by 127·2^−(E1+E3) and cut into FOUR
+//       int8 digits written into 128B-swizzled shared memory — only BN rows
+//       of per-anchor work per n-tile;
+//   acc_k += Σ_{i+j=k} A_i·B_jᵀ for k = 0..3 — nine kind::i8 MMAs per 32
+//       pixels into four int32 TMEM accumulators (terms with i+j ≥ 4 are
+//       below 2^−31 of the leading one).  Per pixel |Σ_{i+j=k}| ≤ 3·127² <
+//       2^15.6, so a chunk of up to 2^15 pixels cannot overflow.
+// Why four digits for the product: its digits are scaled to the bound
+// max|D1|·max|D3|, so three digits leave an error of ~6e-8 of that bound on
+// every pixel, whatever the product's own size.  On sampling-mask maps (a
+// peak at the origin, noise-like sidelobes far below it) those errors add up
+// over the 10^5-10^6 pixels to ~4e-6 of Σ|products|; the fourth digit cuts
+// them by 254.  The plain D2 operand keeps three digits: its error scales
+// with the product it multiplies, which is small wherever D2's own bound is
+// loose.  The k = 3 class matters for the same reason.  Four accumulators of
+// 64 columns plus two 128-pixel A stages (2 × 96 columns) fill TMEM.
 // Epilogue: T = 2^(E1+E2+E3)/127² · Σ_k acc_k·254^−k in FP64,
 // weighted by the channel multiplicities, written to the partial buffer
 // [anchor][chunk][lag2][lag3]; lag_reduce then sums it per lag cell with a
 // compensated FP64 accumulator in a fixed order (deterministic).
 //
-// Warp roles (608 threads): warps 0-15 form A from fp32 D1/D2 tiles that warp
-// 17 stages in shared memory by TMA (3-deep ring, 128B-swizzled so the row
-// reads are conflict-free), and later read the accumulators out; warp 16
-// streams the D3 digit tiles by TMA; warp 18 owns TMEM and issues the MMAs
-// from one lane.
+// Issue rate.  An M=128, N=64 int8 MMA runs ~32 tensor cycles, and the pipe
+// buffers only about two of them, so any latency in a single issuing thread
+// (a barrier test, a commit) leaves it idle.  Two issuing warps, one owning
+// accumulators 0 and 2 and one owning 1 and 3, each issuing its MMAs grouped
+// by accumulator, keep it ~85% busy (measured 37 cycles per MMA against 54
+// for one thread issuing in digit-class order).
+//
+// Warp roles (640 threads): warps 0-7 move the D2 digits from shared memory
+// into TMEM, warps 8-15 form the B digits, warp 16 streams the fp32 D3 tiles
+// and the D1 row by TMA (128B-swizzled, so the row reads are conflict-free),
+// warp 18 streams the D2 digit tiles by TMA, warps 17 and 19 issue the MMAs
+// from one lane each (warp 17 also owns TMEM); warps 0-15 read the
+// accumulators out.
 // Every mbarrier wait is bounded; on expiry the CTA raises an error flag the
 // host turns into AMBER_ERR_TIMEOUT, drains its own copies and MMAs, frees TMEM.
 #include <algorithm>
+#include <cmath>
 #include <vector>
 
 #include "common.cuh"
@@ -50,21 +68,25 @@ namespace {
 
 using namespace tc;
 
-constexpr int BM = 128;        // p2 rows per tile = TMEM lanes
-constexpr int KB_B = 128;      // pixels per B stage: one 128-byte swizzle row of int8
-constexpr int KB_A = 64;       // pixels per A stage in TMEM (two 32-pixel fp32 input boxes)
-constexpr int NSI = 3;         // fp32 input stages in shared memory
-constexpr int NACC = 4;        // int32 accumulators, one per digit class i+j = 0..3
-constexpr int A_STAGE_COLS = 48;  // 3 digits × 16 columns (64 int8 per lane per digit)
-constexpr int NWARP_A = 16;    // A-forming / epilogue warps: 4 warpgroups, 16 pixels each per A stage
-constexpr int WARP_TMA_B = 16;
-constexpr int WARP_TMA_A = 17;
-constexpr int WARP_MMA = 18;
-constexpr int NTHREADS = 19 * 32;
+constexpr int BM = 128;           // p2 rows per tile = TMEM lanes
+constexpr int KB_B = 128;         // pixels per pipeline stage: one 128-byte swizzle row of int8
+constexpr int KB_A = 64;          // pixels per D2 digit tile in shared memory
+constexpr int NACC = 4;           // int32 accumulators, one per digit class i+j = 0..3
+constexpr int A_STAGE_COLS = 96;  // 3 digits × 32 columns (128 int8 per lane per digit)
+constexpr int NSTAGE = 2;         // pipeline stages in flight: A in TMEM, B digits in shared memory
+constexpr int NWARP_A = 8;        // D2-digit movers: 2 warpgroups × 32 pixels of each 64-pixel tile
+constexpr int NWARP_B = 8;        // B formers
+constexpr int WARP_TMA = 16;      // fp32 B inputs
+constexpr int WARP_MMA = 17;      // owns TMEM; MMA issuer 0 (accumulators 0 and 2)
+constexpr int WARP_TMA_A = 18;    // D2 digit tiles
+constexpr int WARP_MMA2 = 19;     // MMA issuer 1 (accumulators 1 and 3)
+constexpr int NISSUE = 2;
+constexpr int NTHREADS = 20 * 32;
 constexpr int TMEM_COLS = 512;
-constexpr int IN_D2 = BM * KB_A * 4;  // bytes of one D2 input stage (two swizzled 32-pixel boxes)
-constexpr int IN_D1 = KB_A * 4;       // bytes of the D1 row of one input stage
-constexpr int IN_STAGE = IN_D2 + 1024;  // D1 row padded to keep 1024-byte alignment
+constexpr int NAS = 4;            // D2 digit tiles in shared memory
+constexpr int NBI = 2;            // fp32 input stages (D3 tile + D1 row)
+constexpr int NDB = 4;            // int8 digits of the per-anchor product (B)
+constexpr int A_BOX = KB_A * BM;  // one digit plane of one D2 tile: 128 rows × 64 bytes, 64B-swizzled
 
 struct ParamsI8 {
     const int *e1, *e2, *e3;  // row exponents [nc]
@@ -78,49 +100,34 @@ struct ParamsI8 {
     int *err;
 };
 
-// Three base-254 digits of t ∈ [−127, 127] (see quantize_kernel in maps.cu):
-// round-to-nearest via the 1.5·2^23 magic number leaves each digit's
-// two's-complement byte in the low mantissa bits.
-__device__ __forceinline__ void digits254(float t, uint32_t &b0, uint32_t &b1, uint32_t &b2)
-{
-    const float M = 12582912.0f;
-    float y0 = t + M;
-    float r0 = (t - (y0 - M)) * 254.f;
-    float y1 = r0 + M;
-    float r1 = (r0 - (y1 - M)) * 254.f;
-    float y2 = r1 + M;
-    b0 = __float_as_uint(y0);
-    b1 = __float_as_uint(y1);
-    b2 = __float_as_uint(y2);
-}
-
-// The same three digits for two products u·v at once, with packed FP32x2
-// arithmetic: every step is one fused op on a pair and the product u·v enters
-// the first rounding unrounded (y0 = fma(u, v, M)).  M − y = −digit exactly.
-__device__ __forceinline__ void digits254x2(float2 u, float2 v, float2 &y0, float2 &y1, float2 &y2)
+// Four base-254 digits of two products u·v at once (packed FP32x2): every
+// step is one fused op on a pair, the product enters the first rounding
+// unrounded (y0 = fma(u, v, M)), and round-to-nearest through the 1.5·2^23
+// magic number leaves each digit's two's-complement byte in the low mantissa
+// bits (as in quantize_kernel, maps.cu).  M − y = −digit exactly, and each
+// residual 254·s − d is exact in FP32 (its lowest bit is at most 2^−22 and
+// it is at most 1/2 in magnitude).
+__device__ __forceinline__ void digits254x2(float2 u, float2 v, float2 &y0, float2 &y1, float2 &y2, float2 &y3)
 {
     const float2 M = make_float2(12582912.0f, 12582912.0f);
     const float2 K254 = make_float2(254.f, 254.f);
     const float2 NEG1 = make_float2(-1.f, -1.f);
-    y0 = __ffma2_rn(u, v, M);                   // M + d0
-    const float2 nq0 = __ffma2_rn(y0, NEG1, M); // −d0
-    const float2 r0 = __ffma2_rn(u, v, nq0);    // u·v − d0
-    y1 = __ffma2_rn(r0, K254, M);               // M + d1
-    const float2 nq1 = __ffma2_rn(y1, NEG1, M); // −d1
-    const float2 s1 = __ffma2_rn(r0, K254, nq1); // 254·r0 − d1
-    y2 = __ffma2_rn(s1, K254, M);               // M + d2
+    y0 = __ffma2_rn(u, v, M);                     // M + d0
+    const float2 nq0 = __ffma2_rn(y0, NEG1, M);   // −d0
+    const float2 r0 = __ffma2_rn(u, v, nq0);      // u·v − d0
+    y1 = __ffma2_rn(r0, K254, M);                 // M + d1
+    const float2 nq1 = __ffma2_rn(y1, NEG1, M);   // −d1
+    const float2 s1 = __ffma2_rn(r0, K254, nq1);  // 254·r0 − d1
+    y2 = __ffma2_rn(s1, K254, M);                 // M + d2
+    const float2 nq2 = __ffma2_rn(y2, NEG1, M);   // −d2
+    const float2 s2 = __ffma2_rn(s1, K254, nq2);  // 254·s1 − d2
+    y3 = __ffma2_rn(s2, K254, M);                 // M + d3
 }
 
-__device__ __forceinline__ uint32_t pack_low_bytes(uint32_t a, uint32_t b, uint32_t c, uint32_t d)
+__device__ __forceinline__ uint32_t pack_low_bytes(float a, float b, float c, float d)
 {
-    return __byte_perm(__byte_perm(a, b, 0x0040), __byte_perm(c, d, 0x0040), 0x5410);
-}
-
-__device__ __forceinline__ void tmem_st4(uint32_t taddr, uint32_t a, uint32_t b, uint32_t c, uint32_t d)
-{
-    asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1, %2, %3, %4};" ::"r"(taddr), "r"(a), "r"(b),
-                 "r"(c), "r"(d)
-                 : "memory");
+    return __byte_perm(__byte_perm(__float_as_uint(a), __float_as_uint(b), 0x0040),
+                       __byte_perm(__float_as_uint(c), __float_as_uint(d), 0x0040), 0x5410);
 }
 
 __device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&v)[8])
@@ -131,34 +138,72 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&v)[8])
                  : "memory");
 }
 
+// kind::i8 MMA, A from TMEM, always accumulating (no predicate set-up on the issue path)
+__device__ __forceinline__ void umma_ts_i8_acc(uint32_t d_tmem, uint32_t a_tmem, uint64_t b_desc, uint32_t idesc)
+{
+    asm volatile("tcgen05.mma.cta_group::1.kind::i8 [%0], [%1], %2, %3, 1;" ::"r"(d_tmem), "r"(a_tmem), "l"(b_desc),
+                 "r"(idesc)
+                 : "memory");
+}
+
+// One issuer's share of a 128-pixel stage: accumulators k = q and q + 2, each fed
+// Σ_{i+j=k} A_i·B_jᵀ (A: 3 digits, B: 4) over the four 32-pixel slices, grouped by accumulator
+// (back-to-back MMAs into one accumulator keep the tensor pipe fullest).
+// The stage's first MMA into each accumulator overwrites it when `fresh`.
+template <int BN>
+__device__ __forceinline__ void issue_stage(uint32_t tmem, uint32_t a_stage, uint64_t b_stage, uint32_t idesc, int q,
+                                            bool fresh)
+{
+    constexpr uint32_t TILE16 = (uint32_t)(BN * KB_B) >> 4;
+#pragma unroll
+    for (int kc = 0; kc < 2; ++kc) {
+        const int k = q + 2 * kc;
+        const uint32_t acc = tmem + (uint32_t)(k * BN);
+        bool first = true;
+#pragma unroll
+        for (int kk = 0; kk < 4; ++kk)
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const int j = k - i;
+                if (j < 0 || j >= NDB) continue;
+                const uint32_t a = a_stage + (uint32_t)(i * 32 + kk * 8);
+                const uint64_t bd = b_stage + (uint64_t)(j * TILE16 + kk * 2);
+                if (first) umma_ts_i8(acc, a, bd, idesc, fresh ? 0u : 1u);
+                else umma_ts_i8_acc(acc, a, bd, idesc);
+                first = false;
+            }
+    }
+}
+
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
 template <int BN>
 __global__ void __launch_bounds__(NTHREADS, 1)
-    contract_i8_kernel(const __grid_constant__ CUtensorMap tm0, const __grid_constant__ CUtensorMap tm1,
-                       const __grid_constant__ CUtensorMap tm2, const __grid_constant__ CUtensorMap tmd2,
-                       const __grid_constant__ CUtensorMap tmd1, const ParamsI8 prm)
+    contract_i8_kernel(const __grid_constant__ CUtensorMap tm_a0, const __grid_constant__ CUtensorMap tm_a1,
+                       const __grid_constant__ CUtensorMap tm_a2, const __grid_constant__ CUtensorMap tm_d3,
+                       const __grid_constant__ CUtensorMap tm_d1, const ParamsI8 prm)
 {
-    constexpr int TILE = BN * KB_B;  // bytes of one digit tile
-    constexpr int STAGE_B = 3 * TILE;
-    // TMEM: the four accumulators take 4·BN columns, the A stages the rest (≤ 4 stages)
+    constexpr int STAGE_BI = BN * KB_B * 4;         // four 32-pixel fp32 boxes of BN rows (the D1 rows sit apart)
+    constexpr int TILE = BN * KB_B;                 // one B digit tile (BN rows × 128 bytes)
+    constexpr int STAGE_BD = NDB * TILE;
     constexpr int A_COL0 = NACC * BN;
-    constexpr int NSA = (TMEM_COLS - A_COL0) / A_STAGE_COLS < 4 ? (TMEM_COLS - A_COL0) / A_STAGE_COLS : 4;
-    constexpr int NSB = ((200 * 1024 - NSI * IN_STAGE) / STAGE_B) < 4 ? ((200 * 1024 - NSI * IN_STAGE) / STAGE_B) : 4;
-    static_assert(NSB >= 2, "shared memory too small for the B stages");
-    static_assert(NSA >= 2, "TMEM must hold at least two A stages");
-    static_assert(A_COL0 + NSA * A_STAGE_COLS <= TMEM_COLS, "A stages must fit in TMEM");
-    static_assert(BN % 32 == 0 && BN >= 32 && BN <= 96, "BN");
+    constexpr int PT = BN / 2;                      // pixels per B-former thread per stage
+    static_assert(BN == 32 || BN == 64, "BN");
+    static_assert(A_COL0 + NSTAGE * A_STAGE_COLS <= TMEM_COLS, "A stages must fit in TMEM");
 
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char *smem = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-    unsigned char *in_tiles = smem;                        // NSI × {D2 box 0, D2 box 1, D1 row}
-    unsigned char *b_tiles = smem + NSI * IN_STAGE;        // NSB × {d0, d1, d2}
-    uint64_t *bars = reinterpret_cast<uint64_t *>(b_tiles + NSB * STAGE_B);
-    uint64_t *b_full = bars, *b_empty = bars + NSB;
-    uint64_t *a_full = bars + 2 * NSB, *a_empty = a_full + NSA;
-    uint64_t *in_full = a_empty + NSA, *in_empty = in_full + NSI;
-    uint64_t *acc_full = in_empty + NSI;
-    uint64_t *drain = acc_full + 1;
-    volatile uint32_t *tmem_slot = reinterpret_cast<volatile uint32_t *>(drain + 1);
+    unsigned char *bin = smem;                       // NBI × STAGE_BI
+    unsigned char *bdig = smem + NBI * STAGE_BI;     // NSTAGE × STAGE_BD
+    unsigned char *atile = bdig + NSTAGE * STAGE_BD;  // NAS × 3 × A_BOX
+    float *d1rows = reinterpret_cast<float *>(atile + NAS * 3 * A_BOX);  // NBI × KB_B fp32: the D1 row of each input stage
+    uint64_t *bars = reinterpret_cast<uint64_t *>(d1rows + NBI * KB_B);
+    uint64_t *as_full = bars, *as_empty = as_full + NAS;
+    uint64_t *bin_full = as_empty + NAS, *bin_empty = bin_full + NBI;
+    uint64_t *st_full = bin_empty + NBI, *st_empty = st_full + NSTAGE;
+    uint64_t *acc_full = st_empty + NSTAGE;
+    uint64_t *drain = acc_full + 1;  // one per issuer
+    volatile uint32_t *tmem_slot = reinterpret_cast<volatile uint32_t *>(drain + NISSUE);
     volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -175,17 +220,18 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     const int p1 = prm.anchors[aidx];
     const long x_begin = (long)chunk * prm.chunk;
     const long x_end = min(prm.k, x_begin + prm.chunk);
-    const int nb = (int)((x_end - x_begin + KB_B - 1) / KB_B);  // B stages; 2 A stages each
-    const int na = 2 * nb;
+    const int nb = (int)((x_end - x_begin + KB_B - 1) / KB_B);  // 128-pixel stages
+    const int na = 2 * nb;                                      // 64-pixel D2 tiles
     const int bbase = p1 - prm.nc10 + nt * BN;                  // first p3 row of the B tile
     const int rbase = p1 - prm.nc10 + mt * BM;                  // first p2 row of the A tile
+    const int E1 = prm.e1[p1];
 
     if (tid == 0) {
-        for (int s = 0; s < NSB; ++s) { mbar_init(&b_full[s], 1); mbar_init(&b_empty[s], 1); }
-        for (int s = 0; s < NSA; ++s) { mbar_init(&a_full[s], NWARP_A); mbar_init(&a_empty[s], 1); }
-        for (int s = 0; s < NSI; ++s) { mbar_init(&in_full[s], 1); mbar_init(&in_empty[s], NWARP_A); }
-        mbar_init(acc_full, 1);
-        mbar_init(drain, 1);
+        for (int s = 0; s < NAS; ++s) { mbar_init(&as_full[s], 1); mbar_init(&as_empty[s], NWARP_A); }
+        for (int s = 0; s < NBI; ++s) { mbar_init(&bin_full[s], 1); mbar_init(&bin_empty[s], NWARP_B); }
+        for (int s = 0; s < NSTAGE; ++s) { mbar_init(&st_full[s], NWARP_A + NWARP_B); mbar_init(&st_empty[s], NISSUE); }
+        mbar_init(acc_full, NISSUE);
+        for (int q = 0; q < NISSUE; ++q) mbar_init(&drain[q], 1);
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -199,153 +245,187 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     __syncthreads();
     fence_after();
     const uint32_t tmem = *tmem_slot;
+    bool ok = true;
 
-    if (warp == WARP_TMA_B) {
-        // B operand: the D3 digit planes, 128 pixels × BN rows per stage
+    if (warp == WARP_TMA) {
+        // fp32 inputs of the B formers: D3 rows [bbase, bbase+BN) as four 32-pixel swizzled boxes, D1 row p1.
+        // Pixels past the end of the map and rows outside [0, nc) come back as zeros.
         if (lane == 0) {
             int issued = 0;
             for (int it = 0; it < nb; ++it) {
-                const int s = it % NSB;
-                if (!mbar_wait(&b_empty[s], ((it / NSB) & 1) ^ 1, abort_flag, prm.err, 1)) break;
-                unsigned char *t0 = b_tiles + s * STAGE_B;
-                mbar_expect_tx(&b_full[s], STAGE_B);
+                const int s = it % NBI;
+                if (!mbar_wait(&bin_empty[s], ((it / NBI) & 1) ^ 1, abort_flag, prm.err, 1)) break;
+                unsigned char *t = bin + s * STAGE_BI;
+                mbar_expect_tx(&bin_full[s], BN * KB_B * 4 + KB_B * 4);
                 const int x = (int)(x_begin + (long)it * KB_B);
-                tma_load_2d(t0, &tm0, &b_full[s], x, bbase);
-                tma_load_2d(t0 + TILE, &tm1, &b_full[s], x, bbase);
-                tma_load_2d(t0 + 2 * TILE, &tm2, &b_full[s], x, bbase);
+#pragma unroll
+                for (int j = 0; j < 4; ++j) tma_load_2d(t + j * (BN * 128), &tm_d3, &bin_full[s], x + 32 * j, bbase);
+                tma_load_2d(d1rows + s * KB_B, &tm_d1, &bin_full[s], x, p1);
                 ++issued;
             }
             if (*abort_flag)
-                for (int it = max(0, issued - NSB); it < issued; ++it)
-                    for (long long i = 0; i < WAIT_LIMIT && !mbar_try_wait(&b_full[it % NSB], (it / NSB) & 1); ++i)
+                for (int it = max(0, issued - NBI); it < issued; ++it)
+                    for (long long i = 0; i < WAIT_LIMIT && !mbar_try_wait(&bin_full[it % NBI], (it / NBI) & 1); ++i)
                         __nanosleep(100);
         }
     } else if (warp == WARP_TMA_A) {
-        // A inputs: 64 pixels of the 128 D2 rows (two swizzled 32-pixel boxes) and of the D1 row.
-        // Pixels past the end of the map come back as zeros, rows outside [0, nc) too.
+        // D2 digit planes, rows [rbase, rbase+128) × 64 pixels per tile; rows outside [0, nc) and
+        // pixels past the end of the map come back as zeros.
         if (lane == 0) {
             int issued = 0;
             for (int ia = 0; ia < na; ++ia) {
-                const int s = ia % NSI;
-                if (!mbar_wait(&in_empty[s], ((ia / NSI) & 1) ^ 1, abort_flag, prm.err, 6)) break;
-                unsigned char *t = in_tiles + s * IN_STAGE;
-                mbar_expect_tx(&in_full[s], IN_D2 + IN_D1);
+                const int s = ia % NAS;
+                if (!mbar_wait(&as_empty[s], ((ia / NAS) & 1) ^ 1, abort_flag, prm.err, 8)) break;
+                unsigned char *t = atile + s * 3 * A_BOX;
+                mbar_expect_tx(&as_full[s], 3 * A_BOX);
                 const int x = (int)(x_begin + (long)ia * KB_A);
-                tma_load_2d(t, &tmd2, &in_full[s], x, rbase);
-                tma_load_2d(t + IN_D2 / 2, &tmd2, &in_full[s], x + 32, rbase);
-                tma_load_2d(t + IN_D2, &tmd1, &in_full[s], x, p1);
+                tma_load_2d(t, &tm_a0, &as_full[s], x, rbase);
+                tma_load_2d(t + A_BOX, &tm_a1, &as_full[s], x, rbase);
+                tma_load_2d(t + 2 * A_BOX, &tm_a2, &as_full[s], x, rbase);
                 ++issued;
             }
             if (*abort_flag)
-                for (int ia = max(0, issued - NSI); ia < issued; ++ia)
-                    for (long long i = 0; i < WAIT_LIMIT && !mbar_try_wait(&in_full[ia % NSI], (ia / NSI) & 1); ++i)
+                for (int ia = max(0, issued - NAS); ia < issued; ++ia)
+                    for (long long i = 0; i < WAIT_LIMIT && !mbar_try_wait(&as_full[ia % NAS], (ia / NAS) & 1); ++i)
                         __nanosleep(100);
         }
-    } else if (warp == WARP_MMA) {
+    } else if (warp == WARP_MMA || warp == WARP_MMA2) {
         if (lane == 0) {
+            const int q = warp == WARP_MMA ? 0 : 1;
             // S32 accumulate, signed int8 A and B, both K-major, M = 128, N = BN
             const uint32_t idesc = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
                                    ((uint32_t)(BM >> 4) << 24);
-            const uint32_t acc0 = tmem, acc1 = tmem + BN, acc2 = tmem + 2 * BN, acc3 = tmem + 3 * BN;
-            // descriptors are linear in the start address (bits 0-13, 16-byte units): build the
-            // first one once and advance it by (byte offset >> 4)
-            const uint64_t desc0 = smem_desc_sw128(smem_u32(b_tiles));
-            bool ok = true;
-            uint32_t started = 0;
-            for (int it = 0; it < nb && ok; ++it) {
-                const int sb = it % NSB;
-                if (!mbar_wait(&b_full[sb], (it / NSB) & 1, abort_flag, prm.err, 2)) { ok = false; break; }
-                const uint64_t dstage = desc0 + (uint64_t)((sb * STAGE_B) >> 4);
-                for (int h = 0; h < 2; ++h) {
-                    const int ia = 2 * it + h, sa = ia % NSA;
-                    if (!mbar_wait(&a_full[sa], (ia / NSA) & 1, abort_flag, prm.err, 3)) { ok = false; break; }
-                    fence_after();
-#pragma unroll
-                    for (int kk = 0; kk < 2; ++kk) {
-                        const uint64_t B0 = dstage + (uint64_t)((2 * h + kk) * 2), B1 = B0 + (TILE >> 4),
-                                       B2 = B0 + (2 * TILE >> 4);
-                        const uint32_t a = tmem + A_COL0 + sa * A_STAGE_COLS + kk * 8;
-                        const uint32_t A0 = a, A1 = a + 16, A2 = a + 32;
-                        umma_ts_i8(acc0, A0, B0, idesc, started);  // i+j = 0
-                        umma_ts_i8(acc1, A0, B1, idesc, started);  // i+j = 1
-                        umma_ts_i8(acc1, A1, B0, idesc, 1u);
-                        umma_ts_i8(acc2, A0, B2, idesc, started);  // i+j = 2
-                        umma_ts_i8(acc2, A1, B1, idesc, 1u);
-                        umma_ts_i8(acc2, A2, B0, idesc, 1u);
-                        umma_ts_i8(acc3, A1, B2, idesc, started);  // i+j = 3
-                        umma_ts_i8(acc3, A2, B1, idesc, 1u);
-                        started = 1u;
-                    }
-                    umma_commit(&a_empty[sa]);
-                }
-                if (ok) umma_commit(&b_empty[sb]);
+            // descriptors are linear in the start address (bits 0-13, 16-byte units)
+            const uint64_t desc0 = smem_desc_sw128(smem_u32(bdig));
+            for (int it = 0; it < nb; ++it) {
+                const int s = it & 1;
+                if (!mbar_wait(&st_full[s], (it >> 1) & 1, abort_flag, prm.err, 2)) { ok = false; break; }
+                fence_after();
+                issue_stage<BN>(tmem, tmem + A_COL0 + s * A_STAGE_COLS, desc0 + (uint64_t)((s * STAGE_BD) >> 4), idesc,
+                                q, it == 0);
+                umma_commit(&st_empty[s]);
             }
             if (ok) {
                 umma_commit(acc_full);
             } else {
-                umma_commit(drain);
-                for (long long i = 0; i < WAIT_LIMIT && !mbar_try_wait(drain, 0); ++i) __nanosleep(100);
+                umma_commit(&drain[q]);
+                for (long long i = 0; i < WAIT_LIMIT && !mbar_try_wait(&drain[q], 0); ++i) __nanosleep(100);
             }
         }
-    } else {
-        // ---- A formation: warps 0-15; warpgroup g covers pixels [16g, 16g + 16) of each A stage ----
+    } else if (warp < NWARP_A) {
+        // ---- D2 digits → TMEM: warpgroup g moves pixels [32g, 32g+32) of each 64-pixel tile ----
+        // Row m of a 64B-swizzled box holds its 16-byte chunk c at position c ^ ((m >> 1) & 3), so
+        // eight consecutive rows reading the same chunk hit eight different bank groups.
         const int g = warp >> 2;
         const int m = ((warp & 3) << 5) + lane;
         const uint32_t lane_field = (uint32_t)((warp & 3) << 5) << 16;
-        const int d2 = mt * BM + m;
-        const int p2 = rbase + m;
-        const bool row_ok = d2 < prm.nclen && p2 >= 0 && p2 < prm.nc && prm.weight[p2] > 0;
-        const int E1 = prm.e1[p1];
-        const int E2 = row_ok ? prm.e2[p2] : 0;
-        const float scale = row_ok ? ldexpf(127.f, -(E1 + E2)) : 0.f;  // A·127·2^−(E1+E2) ∈ [−127, 127]
-        // this thread's 16 pixels: 16-byte chunks j0..j0+3 of one 32-pixel box, 128B-swizzled by row
-        const int box = g >> 1, j0 = (g & 1) * 4;
-        const int px0 = g * 16;
-        bool ok = true;
-        for (int ia = 0; ia < na; ++ia) {
-            const int si = ia % NSI, sa = ia % NSA;
-            if (!mbar_wait_warp(&in_full[si], (ia / NSI) & 1, abort_flag, prm.err, 7)) { ok = false; break; }
-            const unsigned char *t = in_tiles + si * IN_STAGE;
-            const float *rowp = reinterpret_cast<const float *>(t + box * (IN_D2 / 2) + m * 128);
-            const float *d1p = reinterpret_cast<const float *>(t + IN_D2) + px0;
-            uint32_t w[3][4];
-            const float2 sc2 = make_float2(scale, scale);
+        const int sw = (m >> 1) & 3;
+        const int off0 = m * KB_A + (((2 * g) ^ sw) << 4), off1 = m * KB_A + (((2 * g + 1) ^ sw) << 4);
+        // tcgen05.st reads its source registers asynchronously: they are not reused
+        // before tcgen05.wait::st, so the two 64-pixel halves of a stage load into
+        // separate registers, and their shared-memory tiles are released only after
+        // the wait.
+        for (int it = 0; it < nb && ok; ++it) {
+            const int s = it & 1;
+            uint4 r[2][6];
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const float4 v = *reinterpret_cast<const float4 *>(rowp + (((j0 + q) ^ (m & 7)) << 2));
-                const float4 u = *reinterpret_cast<const float4 *>(d1p + 4 * q);
-                float2 ya0, ya1, ya2, yb0, yb1, yb2;
-                digits254x2(__fmul2_rn(make_float2(u.x, u.y), sc2), make_float2(v.x, v.y), ya0, ya1, ya2);
-                digits254x2(__fmul2_rn(make_float2(u.z, u.w), sc2), make_float2(v.z, v.w), yb0, yb1, yb2);
-                w[0][q] = pack_low_bytes(__float_as_uint(ya0.x), __float_as_uint(ya0.y), __float_as_uint(yb0.x),
-                                         __float_as_uint(yb0.y));
-                w[1][q] = pack_low_bytes(__float_as_uint(ya1.x), __float_as_uint(ya1.y), __float_as_uint(yb1.x),
-                                         __float_as_uint(yb1.y));
-                w[2][q] = pack_low_bytes(__float_as_uint(ya2.x), __float_as_uint(ya2.y), __float_as_uint(yb2.x),
-                                         __float_as_uint(yb2.y));
+            for (int h = 0; h < 2; ++h) {
+                const int ia = 2 * it + h, sa = ia % NAS;
+                if (!mbar_wait_warp(&as_full[sa], (ia / NAS) & 1, abort_flag, prm.err, 9)) { ok = false; break; }
+                const unsigned char *t = atile + sa * 3 * A_BOX;
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    r[h][2 * d] = *reinterpret_cast<const uint4 *>(t + d * A_BOX + off0);
+                    r[h][2 * d + 1] = *reinterpret_cast<const uint4 *>(t + d * A_BOX + off1);
+                }
             }
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&in_empty[si]);
-            if (!mbar_wait_warp(&a_empty[sa], ((ia / NSA) & 1) ^ 1, abort_flag, prm.err, 4)) { ok = false; break; }
+            if (!ok) break;
+            if (!mbar_wait_warp(&st_empty[s], ((it >> 1) & 1) ^ 1, abort_flag, prm.err, 4)) { ok = false; break; }
             fence_after();
-            const uint32_t col = tmem + lane_field + A_COL0 + sa * A_STAGE_COLS + g * 4;
-            tmem_st4(col, w[0][0], w[0][1], w[0][2], w[0][3]);
-            tmem_st4(col + 16, w[1][0], w[1][1], w[1][2], w[1][3]);
-            tmem_st4(col + 32, w[2][0], w[2][1], w[2][2], w[2][3]);
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                // 32-pixel slice kk = 2h + g of the stage: columns 8·kk .. 8·kk+7 of each digit's 32
+                const uint32_t col = tmem + lane_field + A_COL0 + s * A_STAGE_COLS + (2 * h + g) * 8;
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    const uint32_t v[8] = {r[h][2 * d].x,     r[h][2 * d].y,     r[h][2 * d].z,     r[h][2 * d].w,
+                                           r[h][2 * d + 1].x, r[h][2 * d + 1].y, r[h][2 * d + 1].z, r[h][2 * d + 1].w};
+                    tmem_st8(col + 32 * d, v);
+                }
+            }
             asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
             fence_before();
             __syncwarp();
-            if (lane == 0) mbar_arrive(&a_full[sa]);
+            if (lane == 0) {
+                mbar_arrive(&as_empty[(2 * it) % NAS]);
+                mbar_arrive(&as_empty[(2 * it + 1) % NAS]);
+                mbar_arrive(&st_full[s]);
+            }
         }
+    } else if (warp < NWARP_A + NWARP_B) {
+        // ---- B formers: thread (row n, segment sg) forms PT pixels of D1[p1]·D3[bbase+n] per stage ----
+        const int tb = tid - NWARP_A * 32;  // 0..255
+        const int n = tb % BN, sg = tb / BN;
+        const int px0 = sg * PT;  // first pixel of this thread inside the 128-pixel stage
+        const int p3 = bbase + n;
+        const bool col_ok = p3 >= 0 && p3 < prm.nc;
+        const float scale = col_ok ? ldexpf(127.f, -(E1 + prm.e3[p3])) : 0.f;
+        const float2 sc2 = make_float2(scale, scale);
+        const int box = px0 / 32, c0 = (px0 % 32) / 4;  // input box and first 16-byte chunk in it
+        for (int it = 0; it < nb; ++it) {
+            const int si = it % NBI, s = it & 1;
+            if (!mbar_wait_warp(&bin_full[si], (it / NBI) & 1, abort_flag, prm.err, 6)) { ok = false; break; }
+            const unsigned char *t = bin + si * STAGE_BI;
+            const unsigned char *rowp = t + box * (BN * 128) + n * 128;
+            const float *d1p = d1rows + si * KB_B + px0;
+            uint32_t w[NDB][PT / 4];
+#pragma unroll
+            for (int q = 0; q < PT / 4; ++q) {
+                const float4 v = *reinterpret_cast<const float4 *>(rowp + (((c0 + q) ^ (n & 7)) << 4));
+                const float4 u = *reinterpret_cast<const float4 *>(d1p + 4 * q);
+                float2 ya0, ya1, ya2, ya3, yb0, yb1, yb2, yb3;
+                digits254x2(__fmul2_rn(make_float2(u.x, u.y), sc2), make_float2(v.x, v.y), ya0, ya1, ya2, ya3);
+                digits254x2(__fmul2_rn(make_float2(u.z, u.w), sc2), make_float2(v.z, v.w), yb0, yb1, yb2, yb3);
+                w[0][q] = pack_low_bytes(ya0.x, ya0.y, yb0.x, yb0.y);
+                w[1][q] = pack_low_bytes(ya1.x, ya1.y, yb1.x, yb1.y);
+                w[2][q] = pack_low_bytes(ya2.x, ya2.y, yb2.x, yb2.y);
+                w[3][q] = pack_low_bytes(ya3.x, ya3.y, yb3.x, yb3.y);
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&bin_empty[si]);
+            if (!mbar_wait_warp(&st_empty[s], ((it >> 1) & 1) ^ 1, abort_flag, prm.err, 7)) { ok = false; break; }
+            unsigned char *dst = bdig + s * STAGE_BD + n * 128;
+#pragma unroll
+            for (int d = 0; d < NDB; ++d)
+#pragma unroll
+                for (int q = 0; q < PT / 16; ++q) {
+                    const int cc = px0 / 16 + q;
+                    *reinterpret_cast<uint4 *>(dst + d * TILE + ((cc ^ (n & 7)) << 4)) =
+                        make_uint4(w[d][4 * q], w[d][4 * q + 1], w[d][4 * q + 2], w[d][4 * q + 3]);
+                }
+            fence_proxy_async_smem();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&st_full[s]);
+        }
+    }
 
-        // ---- epilogue: int32 digit accumulators → FP64 partial tile; warpgroup g reads BN/4 columns ----
-        if (ok && mbar_wait_warp(acc_full, 0, abort_flag, prm.err, 5)) {
+    // ---- epilogue (warps 0-15): int32 digit accumulators → FP64 partial tile; warpgroup wg reads BN/4 columns ----
+    if (warp < NWARP_A + NWARP_B) {
+        const int wg = warp >> 2;
+        const int m = ((warp & 3) << 5) + lane;
+        const uint32_t lane_field = (uint32_t)((warp & 3) << 5) << 16;
+        const bool good = __all_sync(0xffffffffu, ok) && mbar_wait_warp(acc_full, 0, abort_flag, prm.err, 5);
+        if (good) {
             fence_after();
+            const int d2 = mt * BM + m;
+            const int p2 = rbase + m;
+            const bool row_ok = d2 < prm.nclen && p2 >= 0 && p2 < prm.nc && prm.weight[p2] > 0;
+            const int E12 = E1 + (row_ok ? prm.e2[p2] : 0);
             const double wr = row_ok ? (double)prm.weight[p1] * (double)prm.weight[p2] : 0.0;
             double *dst = nullptr;
             if (d2 < prm.nclen)
                 dst = prm.partial + ((long)aidx * prm.nchunk + chunk) * prm.nclen * prm.nclen + (long)d2 * prm.nclen;
-            const int c_begin = g * (BN / 4), c_end = c_begin + BN / 4;
+            const int c_begin = wg * (BN / 4), c_end = c_begin + BN / 4;
             const double i254 = 1.0 / 254.0, i254_2 = i254 * i254, i254_3 = i254_2 * i254;
             for (int c0 = c_begin; c0 < c_end; c0 += 8) {
                 uint32_t v0[8], v1[8], v2[8], v3[8];
@@ -357,15 +437,15 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                 if (dst) {
 #pragma unroll
                     for (int j = 0; j < 8; ++j) {
-                        const int n = c0 + j;
-                        const int d3 = nt * BN + n;
+                        const int nn = c0 + j;
+                        const int d3 = nt * BN + nn;
                         if (d3 >= prm.nclen) continue;
-                        const int p3 = bbase + n;
+                        const int p3 = bbase + nn;
                         double val = 0.0;
                         if (wr != 0.0 && p3 >= 0 && p3 < prm.nc && prm.weight[p3] > 0) {
                             const double s = (double)(int)v0[j] + (double)(int)v1[j] * i254 +
                                              (double)(int)v2[j] * i254_2 + (double)(int)v3[j] * i254_3;
-                            val = ldexp(s * (1.0 / 16129.0), E1 + E2 + prm.e3[p3]) * wr * (double)prm.weight[p3];
+                            val = ldexp(s * (1.0 / 16129.0), E12 + prm.e3[p3]) * wr * (double)prm.weight[p3];
                         }
                         dst[d3] = val;
                     }
@@ -383,11 +463,10 @@ __global__ void __launch_bounds__(NTHREADS, 1)
 }
 
 template <int BN>
-size_t smem_bytes()  // NSB as in the kernel
+size_t smem_bytes()
 {
-    constexpr int STAGE_B = 3 * BN * KB_B;
-    constexpr int NSB = ((200 * 1024 - NSI * IN_STAGE) / STAGE_B) < 4 ? ((200 * 1024 - NSI * IN_STAGE) / STAGE_B) : 4;
-    return 1024 + (size_t)NSI * IN_STAGE + (size_t)NSB * STAGE_B + 256;
+    return 1024 + (size_t)NBI * BN * KB_B * 4 + (size_t)NSTAGE * NDB * BN * KB_B + (size_t)NAS * 3 * A_BOX +
+           (size_t)NBI * KB_B * 4 + 256;
 }
 
 typedef CUresult (*EncodeTiled)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
@@ -416,17 +495,41 @@ int encode(amber_cuda_ctx *c, CUtensorMap *m, CUtensorMapDataType dt, const void
 }
 
 template <int BN>
-int launch(amber_cuda_ctx *c, const CUtensorMap &t0, const CUtensorMap &t1, const CUtensorMap &t2,
-           const CUtensorMap &td2, const CUtensorMap &td1, const ParamsI8 &prm, long items)
+int launch(amber_cuda_ctx *c, const CUtensorMap (&ta)[3], const CUtensorMap &td3, const CUtensorMap &td1,
+           const ParamsI8 &prm, long items)
 {
     const size_t sm = smem_bytes<BN>();
     cudaFuncSetAttribute(contract_i8_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     phase_begin(c, 1);
-    contract_i8_kernel<BN><<<(unsigned)items, NTHREADS, sm, c->stream>>>(t0, t1, t2, td2, td1, prm);
+    contract_i8_kernel<BN><<<(unsigned)items, NTHREADS, sm, c->stream>>>(ta[0], ta[1], ta[2], td3, td1, prm);
     phase_end(c);
     c->launches += 1;
     c->contractions += 1;
     return cuda_check(c, cudaGetLastError(), "contract_i8_kernel launch");
+}
+
+// Pixel chunks per (anchor, tile) pair.  One CTA runs per SM, so the launch
+// takes ceil(items / SMs) rounds of one chunk each; more chunks shorten a
+// round but add a fixed cost per CTA (pipeline fill, epilogue) and partial
+// tiles for lag_reduce to read.  Picks the count with the least modelled time.
+long choose_chunks(long k, long pairs, int sms, long ncsize, long max_chunk)
+{
+    const long nch_min = std::max<long>(1, (k + max_chunk - 1) / max_chunk);
+    const long nch_max = std::max<long>(nch_min, std::min<long>(4 * nch_min + 16, (k + 1023) / 1024));
+    const double stage_s = 0.65e-6;     // one 128-pixel stage of one CTA
+    const double fixed_s = 6 * stage_s;  // fill, drain and epilogue of one CTA
+    const double reduce_bw = 5e12;      // bytes/s for lag_reduce reading the partial tiles
+    long best = nch_min;
+    double best_t = 1e300;
+    for (long nch = nch_min; nch <= nch_max; ++nch) {
+        const long chunk = ((k + nch - 1) / nch + KB_B - 1) / KB_B * KB_B;
+        const long n = (k + chunk - 1) / chunk;
+        if (n != nch) continue;
+        const double rounds = std::ceil((double)(pairs * n) / sms);
+        const double t = rounds * ((double)(chunk / KB_B) * stage_s + fixed_s) + 8.0 * pairs * n * ncsize / reduce_bw;
+        if (t < best_t) { best_t = t; best = n; }
+    }
+    return best;
 }
 
 }  // namespace
@@ -439,16 +542,13 @@ int contract_i8(amber_cuda_ctx *c, const DigitMaps &m1, const DigitMaps &m2, con
     const int nA = (int)c->anchors.size();
     if (nA == 0) return cuda_check(c, cudaMemsetAsync(lag_out, 0, sizeof(double) * ncsize, c->stream), "zero lag");
     const int MT = (nclen + BM - 1) / BM;
-    const int NT = (nclen + 95) / 96;
-    const int BN = ((nclen + NT - 1) / NT + 31) / 32 * 32;
+    const int BN = nclen <= 32 ? 32 : 64;
+    const int NT = (nclen + BN - 1) / BN;
     const long base_items = (long)nA * MT * NT;
-    const long target = 4L * c->num_sms;
     long max_chunk = c->chunk_px > 0 ? std::min<long>(c->chunk_px, 32768) : 32768;
     max_chunk = std::max<long>(KB_B, max_chunk / KB_B * KB_B);
-    long nch = std::max<long>((k + max_chunk - 1) / max_chunk,
-                              std::min<long>((target + base_items - 1) / base_items, (k + 1023) / 1024));
-    nch = std::max<long>(nch, 1);
-    long chunk = ((k + nch - 1) / nch + KB_B - 1) / KB_B * KB_B;
+    long nch = choose_chunks(k, base_items, c->num_sms, ncsize, max_chunk);
+    const long chunk = ((k + nch - 1) / nch + KB_B - 1) / KB_B * KB_B;
     nch = (k + chunk - 1) / chunk;
 
     int rc;
@@ -458,13 +558,13 @@ int contract_i8(amber_cuda_ctx *c, const DigitMaps &m1, const DigitMaps &m2, con
     int *d_err = (int *)c->misc.p;
     if ((rc = cuda_check(c, cudaMemsetAsync(d_err, 0, sizeof(int), c->stream), "error flag"))) return rc;
 
-    CUtensorMap t0, t1, t2, td2, td1;
+    CUtensorMap ta[3], td3, td1;
     const CUtensorMapDataType u8 = CU_TENSOR_MAP_DATA_TYPE_UINT8, f32 = CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
-    if ((rc = encode(c, &t0, u8, m3.d0, k, kp, c->nc, KB_B, BN, CU_TENSOR_MAP_SWIZZLE_128B))) return rc;
-    if ((rc = encode(c, &t1, u8, m3.d1, k, kp, c->nc, KB_B, BN, CU_TENSOR_MAP_SWIZZLE_128B))) return rc;
-    if ((rc = encode(c, &t2, u8, m3.d2, k, kp, c->nc, KB_B, BN, CU_TENSOR_MAP_SWIZZLE_128B))) return rc;
-    if ((rc = encode(c, &td2, f32, m2.f32, k, kp * 4, c->nc, 32, BM, CU_TENSOR_MAP_SWIZZLE_128B))) return rc;
-    if ((rc = encode(c, &td1, f32, m1.f32, k, kp * 4, c->nc, KB_A, 1, CU_TENSOR_MAP_SWIZZLE_NONE))) return rc;
+    const int8_t *planes[3] = {m2.d0, m2.d1, m2.d2};
+    for (int d = 0; d < 3; ++d)
+        if ((rc = encode(c, &ta[d], u8, planes[d], k, kp, c->nc, KB_A, BM, CU_TENSOR_MAP_SWIZZLE_64B))) return rc;
+    if ((rc = encode(c, &td3, f32, m3.f32, k, kp * 4, c->nc, 32, BN, CU_TENSOR_MAP_SWIZZLE_128B))) return rc;
+    if ((rc = encode(c, &td1, f32, m1.f32, k, kp * 4, c->nc, KB_B, 1, CU_TENSOR_MAP_SWIZZLE_NONE))) return rc;
     ParamsI8 prm{};
     prm.nanchors = nA;
     prm.e1 = m1.expo; prm.e2 = m2.expo; prm.e3 = m3.expo;
@@ -477,9 +577,8 @@ int contract_i8(amber_cuda_ctx *c, const DigitMaps &m1, const DigitMaps &m2, con
     prm.err = d_err;
     const long items = base_items * nch;
     switch (BN) {
-        case 32: rc = launch<32>(c, t0, t1, t2, td2, td1, prm, items); break;
-        case 64: rc = launch<64>(c, t0, t1, t2, td2, td1, prm, items); break;
-        case 96: rc = launch<96>(c, t0, t1, t2, td2, td1, prm, items); break;
+        case 32: rc = launch<32>(c, ta, td3, td1, prm, items); break;
+        case 64: rc = launch<64>(c, ta, td3, td1, prm, items); break;
         default: rc = fail(c, AMBER_ERR_ARG, "no int8 tile configuration for nclen=%d (BN=%d)", nclen, BN);
     }
     if (rc) return rc;

@@ -77,7 +77,9 @@ __device__ __forceinline__ bool mbar_wait_warp(uint64_t *bar, uint32_t parity, v
 {
     int ok = 0;
     if ((threadIdx.x & 31) == 0) ok = mbar_wait(bar, parity, abort_flag, err, code) ? 1 : 0;
-    return __shfl_sync(0xffffffffu, ok, 0) != 0;
+    ok = __shfl_sync(0xffffffffu, ok, 0);
+    __syncwarp();  // orders lane 0's acquire before the other lanes' reads of the guarded data
+    return ok != 0;
 }
 
 __device__ __forceinline__ void mbar_arrive(uint64_t *bar)

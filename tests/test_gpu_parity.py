@@ -82,6 +82,38 @@ def test_estimator_vs_oracle(precision, nn, nc, nbins, hi, nc10, flagged, seed, 
         assert ei.max() <= tol, ei.max()
 
 
+def test_mixed_vs_fp64_full_size(lib_built):
+    """The single-realisation workload (256² grid, 128 channels, 16 bins) at full size: the
+    mixed path against the FP64 path on the same GPU, per lag cell, scaled by Σ|products|
+    (the FP64 path with |D| maps).  Covers the largest maps (Ng1 = 740, 5.5e5 pixels), where
+    the sampling-mask sums are dominated by one peak pixel and the digit errors of every
+    other pixel add up; plus a spread of smaller triangles."""
+    import amber_b200
+    real = synth.config2(seed=1)
+    with amber_b200.Estimator(precision="mixed") as est:
+        est.load_grid(real.gv, real.counts, real.du, real.flag_key)
+        est.set_rings(real.ulow, real.uhigh)
+        est.set_channels(real.nc10, real.uf_chans)
+        tri = est.calcr()[:, :3].astype(np.int32)
+        sample = np.concatenate([tri[::31], tri[-3:]])
+        est.run(sample, want_v2=True)
+        m_bl, _, m_nt = est.fetch(want_v2=True)
+    out = {}
+    for prec in ("fp64", "fp64_abs"):
+        with amber_b200.Estimator(precision=prec) as e64:
+            e64.load_grid(real.gv, real.counts, real.du, real.flag_key)
+            e64.set_rings(real.ulow, real.uhigh)
+            e64.set_channels(real.nc10, real.uf_chans)
+            e64.run(sample, want_v2=True)
+            out[prec] = e64.fetch(want_v2=True)
+    (bl, _, nt), (abl, _, ant) = out["fp64"], out["fp64_abs"]
+    ed = (np.abs(m_bl - bl) / (abl + 1e-300)).reshape(len(sample), -1).max(axis=1)
+    ei = (np.abs(m_nt - nt) / (ant + 1e-300)).reshape(len(sample), -1).max(axis=1)
+    print("max rel err per triangle, D sums:", ed, "mask sums:", ei)
+    assert ed.max() <= TOL["mixed"], (sample[int(ed.argmax())], ed.max())
+    assert ei.max() <= TOL["mixed"], (sample[int(ei.argmax())], ei.max())
+
+
 def test_triangle_v1_v2_file_scalars(lib_built):
     import amber_b200
     z = np.load(os.path.join(GOLDEN, "est_flagged48.npz"))
