@@ -47,12 +47,12 @@
 // by accumulator, keep it ~85% busy (measured 37 cycles per MMA against 54
 // for one thread issuing in digit-class order).
 //
-// Warp roles (640 threads): warps 0-7 move the D2 digits from shared memory
-// into TMEM, warps 8-15 form the B digits, warp 16 streams the fp32 D3 tiles
-// and the D1 row by TMA (128B-swizzled, so the row reads are conflict-free),
-// warp 18 streams the D2 digit tiles by TMA, warps 17 and 19 issue the MMAs
-// from one lane each (warp 17 also owns TMEM); warps 0-15 read the
-// accumulators out.
+// Warp roles (768 threads): warps 0-3 move the D2 digits from shared memory
+// into TMEM (one warp per 32 TMEM lanes), warps 4-19 form the B digits, warp
+// 20 streams the fp32 D3 tiles and the D1 row by TMA (128B-swizzled, so the
+// row reads are conflict-free), warp 22 streams the D2 digit tiles by TMA,
+// warps 21 and 23 issue the MMAs from one lane each (warp 21 also owns
+// TMEM); warps 0-15 read the accumulators out.
 // Every mbarrier wait is bounded; on expiry the CTA raises an error flag the
 // host turns into AMBER_ERR_TIMEOUT, drains its own copies and MMAs, frees TMEM.
 #include <algorithm>
@@ -74,14 +74,15 @@ constexpr int KB_A = 64;          // pixels per D2 digit tile in shared memory
 constexpr int NACC = 4;           // int32 accumulators, one per digit class i+j = 0..3
 constexpr int A_STAGE_COLS = 96;  // 3 digits × 32 columns (128 int8 per lane per digit)
 constexpr int NSTAGE = 2;         // pipeline stages in flight: A in TMEM, B digits in shared memory
-constexpr int NWARP_A = 8;        // D2-digit movers: 2 warpgroups × 32 pixels of each 64-pixel tile
-constexpr int NWARP_B = 8;        // B formers
-constexpr int WARP_TMA = 16;      // fp32 B inputs
-constexpr int WARP_MMA = 17;      // owns TMEM; MMA issuer 0 (accumulators 0 and 2)
-constexpr int WARP_TMA_A = 18;    // D2 digit tiles
-constexpr int WARP_MMA2 = 19;     // MMA issuer 1 (accumulators 1 and 3)
+constexpr int NWARP_A = 4;        // D2-digit movers: one warp per 32 TMEM lanes
+constexpr int NWARP_B = 16;       // B formers
+constexpr int WARP_TMA = 20;      // fp32 B inputs
+constexpr int WARP_MMA = 21;      // owns TMEM; MMA issuer 0 (accumulators 0 and 2)
+constexpr int WARP_TMA_A = 22;    // D2 digit tiles
+constexpr int WARP_MMA2 = 23;     // MMA issuer 1 (accumulators 1 and 3)
+constexpr int NEPI = 16;          // epilogue warps (movers and the first formers): 4 warpgroups
 constexpr int NISSUE = 2;
-constexpr int NTHREADS = 20 * 32;
+constexpr int NTHREADS = 24 * 32;
 constexpr int TMEM_COLS = 512;
 constexpr int NAS = 4;            // D2 digit tiles in shared memory
 constexpr int NBI = 2;            // fp32 input stages (D3 tile + D1 row)
@@ -187,9 +188,11 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     constexpr int TILE = BN * KB_B;                 // one B digit tile (BN rows × 128 bytes)
     constexpr int STAGE_BD = NDB * TILE;
     constexpr int A_COL0 = NACC * BN;
-    constexpr int PT = BN / 2;                      // pixels per B-former thread per stage
+    constexpr int PT = BN * KB_B / (NWARP_B * 32);  // pixels per B-former thread per stage (16 or 8)
     static_assert(BN == 32 || BN == 64, "BN");
     static_assert(A_COL0 + NSTAGE * A_STAGE_COLS <= TMEM_COLS, "A stages must fit in TMEM");
+    static_assert(PT == 16 || PT == 8, "former pixels per thread");
+    static_assert(NWARP_A == 4 && NEPI <= NWARP_A + NWARP_B, "warp roles");
 
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char *smem = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -313,58 +316,49 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             }
         }
     } else if (warp < NWARP_A) {
-        // ---- D2 digits → TMEM: warpgroup g moves pixels [32g, 32g+32) of each 64-pixel tile ----
+        // ---- D2 digits → TMEM: warp w moves TMEM lanes [32w, 32w+32), all 64 pixels of each tile ----
         // Row m of a 64B-swizzled box holds its 16-byte chunk c at position c ^ ((m >> 1) & 3), so
         // eight consecutive rows reading the same chunk hit eight different bank groups.
-        const int g = warp >> 2;
-        const int m = ((warp & 3) << 5) + lane;
-        const uint32_t lane_field = (uint32_t)((warp & 3) << 5) << 16;
+        // tcgen05.st reads its source registers asynchronously: they are not reused before
+        // tcgen05.wait::st, and a tile's shared memory is released only after that wait.
+        const int m = (warp << 5) + lane;
+        const uint32_t lane_field = (uint32_t)(warp << 5) << 16;
         const int sw = (m >> 1) & 3;
-        const int off0 = m * KB_A + (((2 * g) ^ sw) << 4), off1 = m * KB_A + (((2 * g + 1) ^ sw) << 4);
-        // tcgen05.st reads its source registers asynchronously: they are not reused
-        // before tcgen05.wait::st, so the two 64-pixel halves of a stage load into
-        // separate registers, and their shared-memory tiles are released only after
-        // the wait.
         for (int it = 0; it < nb && ok; ++it) {
             const int s = it & 1;
-            uint4 r[2][6];
-#pragma unroll
+#pragma unroll 1
             for (int h = 0; h < 2; ++h) {
                 const int ia = 2 * it + h, sa = ia % NAS;
                 if (!mbar_wait_warp(&as_full[sa], (ia / NAS) & 1, abort_flag, prm.err, 9)) { ok = false; break; }
-                const unsigned char *t = atile + sa * 3 * A_BOX;
+                const unsigned char *t = atile + sa * 3 * A_BOX + m * KB_A;
+                uint32_t v[3][16];
 #pragma unroll
-                for (int d = 0; d < 3; ++d) {
-                    r[h][2 * d] = *reinterpret_cast<const uint4 *>(t + d * A_BOX + off0);
-                    r[h][2 * d + 1] = *reinterpret_cast<const uint4 *>(t + d * A_BOX + off1);
+                for (int d = 0; d < 3; ++d)
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) {
+                        const uint4 x = *reinterpret_cast<const uint4 *>(t + d * A_BOX + ((c ^ sw) << 4));
+                        v[d][4 * c] = x.x; v[d][4 * c + 1] = x.y; v[d][4 * c + 2] = x.z; v[d][4 * c + 3] = x.w;
+                    }
+                if (h == 0) {
+                    if (!mbar_wait_warp(&st_empty[s], ((it >> 1) & 1) ^ 1, abort_flag, prm.err, 4)) { ok = false; break; }
+                    fence_after();
                 }
+                // pixels 64h .. 64h+63 of the stage = 32-pixel slices 2h, 2h+1: columns 16h .. 16h+15 of each digit
+                const uint32_t col = tmem + lane_field + A_COL0 + s * A_STAGE_COLS + 16 * h;
+#pragma unroll
+                for (int d = 0; d < 3; ++d) tmem_st16(col + 32 * d, v[d]);
+                asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&as_empty[sa]);
             }
             if (!ok) break;
-            if (!mbar_wait_warp(&st_empty[s], ((it >> 1) & 1) ^ 1, abort_flag, prm.err, 4)) { ok = false; break; }
-            fence_after();
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                // 32-pixel slice kk = 2h + g of the stage: columns 8·kk .. 8·kk+7 of each digit's 32
-                const uint32_t col = tmem + lane_field + A_COL0 + s * A_STAGE_COLS + (2 * h + g) * 8;
-#pragma unroll
-                for (int d = 0; d < 3; ++d) {
-                    const uint32_t v[8] = {r[h][2 * d].x,     r[h][2 * d].y,     r[h][2 * d].z,     r[h][2 * d].w,
-                                           r[h][2 * d + 1].x, r[h][2 * d + 1].y, r[h][2 * d + 1].z, r[h][2 * d + 1].w};
-                    tmem_st8(col + 32 * d, v);
-                }
-            }
-            asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
             fence_before();
             __syncwarp();
-            if (lane == 0) {
-                mbar_arrive(&as_empty[(2 * it) % NAS]);
-                mbar_arrive(&as_empty[(2 * it + 1) % NAS]);
-                mbar_arrive(&st_full[s]);
-            }
+            if (lane == 0) mbar_arrive(&st_full[s]);
         }
     } else if (warp < NWARP_A + NWARP_B) {
         // ---- B formers: thread (row n, segment sg) forms PT pixels of D1[p1]·D3[bbase+n] per stage ----
-        const int tb = tid - NWARP_A * 32;  // 0..255
+        const int tb = tid - NWARP_A * 32;  // 0 .. 32·NWARP_B − 1
         const int n = tb % BN, sg = tb / BN;
         const int px0 = sg * PT;  // first pixel of this thread inside the 128-pixel stage
         const int p3 = bbase + n;
@@ -372,11 +366,13 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         const float scale = col_ok ? ldexpf(127.f, -(E1 + prm.e3[p3])) : 0.f;
         const float2 sc2 = make_float2(scale, scale);
         const int box = px0 / 32, c0 = (px0 % 32) / 4;  // input box and first 16-byte chunk in it
+        // destination: 16-byte chunk px0/16 of each 128-byte digit row, at its swizzled position; PT = 8
+        // fills one half of it
+        const int dst_off = n * 128 + (((px0 / 16) ^ (n & 7)) << 4) + (px0 % 16);
         for (int it = 0; it < nb; ++it) {
             const int si = it % NBI, s = it & 1;
             if (!mbar_wait_warp(&bin_full[si], (it / NBI) & 1, abort_flag, prm.err, 6)) { ok = false; break; }
-            const unsigned char *t = bin + si * STAGE_BI;
-            const unsigned char *rowp = t + box * (BN * 128) + n * 128;
+            const unsigned char *rowp = bin + si * STAGE_BI + box * (BN * 128) + n * 128;
             const float *d1p = d1rows + si * KB_B + px0;
             uint32_t w[NDB][PT / 4];
 #pragma unroll
@@ -394,15 +390,14 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             __syncwarp();
             if (lane == 0) mbar_arrive(&bin_empty[si]);
             if (!mbar_wait_warp(&st_empty[s], ((it >> 1) & 1) ^ 1, abort_flag, prm.err, 7)) { ok = false; break; }
-            unsigned char *dst = bdig + s * STAGE_BD + n * 128;
+            unsigned char *dst = bdig + s * STAGE_BD + dst_off;
 #pragma unroll
-            for (int d = 0; d < NDB; ++d)
-#pragma unroll
-                for (int q = 0; q < PT / 16; ++q) {
-                    const int cc = px0 / 16 + q;
-                    *reinterpret_cast<uint4 *>(dst + d * TILE + ((cc ^ (n & 7)) << 4)) =
-                        make_uint4(w[d][4 * q], w[d][4 * q + 1], w[d][4 * q + 2], w[d][4 * q + 3]);
-                }
+            for (int d = 0; d < NDB; ++d) {
+                if constexpr (PT == 16)
+                    *reinterpret_cast<uint4 *>(dst + d * TILE) = make_uint4(w[d][0], w[d][1], w[d][2], w[d][3]);
+                else
+                    *reinterpret_cast<uint2 *>(dst + d * TILE) = make_uint2(w[d][0], w[d][1]);
+            }
             fence_proxy_async_smem();
             __syncwarp();
             if (lane == 0) mbar_arrive(&st_full[s]);
@@ -410,7 +405,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     }
 
     // ---- epilogue (warps 0-15): int32 digit accumulators → FP64 partial tile; warpgroup wg reads BN/4 columns ----
-    if (warp < NWARP_A + NWARP_B) {
+    if (warp < NEPI) {
         const int wg = warp >> 2;
         const int m = ((warp & 3) << 5) + lane;
         const uint32_t lane_field = (uint32_t)((warp & 3) << 5) << 16;
