@@ -256,7 +256,7 @@ void amber_cuda_destroy(amber_cuda_ctx *c)
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);
     DevBuf *bufs[] = {&c->grid, &c->mask, &c->d_weight, &c->d_anchors, &c->y, &c->maps_d, &c->maps_i,
-                      &c->partial, &c->results, &c->ring_lohi, &c->misc, &c->mixed_scratch};
+                      &c->partial, &c->results, &c->ring_lohi, &c->misc, &c->mixed_scratch, &c->lagred};
     for (DevBuf *b : bufs) release(c, *b);
     for (auto &kv : c->twiddles) release(c, kv.second);
     for (auto &e : c->phase_ev) {

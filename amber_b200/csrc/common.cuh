@@ -75,6 +75,7 @@ struct amber_cuda_ctx {
     amber::DevBuf ring_lohi;
     amber::DevBuf misc;
     amber::DevBuf mixed_scratch;
+    amber::DevBuf lagred;  // two-pass lag reduction: per-group sums and compensations
 
     // per-phase device timing of the last run (CUDA events on the launch stream)
     struct PhaseEv {

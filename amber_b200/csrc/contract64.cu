@@ -13,8 +13,8 @@
 // 4 × 4 register block per thread in FP64.  Channel multiplicities
 // (flagging) weight the tile when it is written.  Tiles go to a partial
 // buffer [anchor][k-split][lag2][lag3]; lag_reduce sums that buffer per lag
-// cell in a fixed order with a compensated (TwoSum) accumulator, so results
-// are deterministic and independent of the launch shape.
+// cell in a fixed grouping and order with compensated (TwoSum) accumulators,
+// so results are deterministic.
 #include <algorithm>
 
 #include "common.cuh"
@@ -133,19 +133,41 @@ __global__ void __launch_bounds__(256) contract64_kernel(const double *__restric
     }
 }
 
-// lag[d] = Σ_{u < nunits} partial[u][d], TwoSum-compensated, fixed order.
-__global__ void lag_reduce_kernel(const double *__restrict__ partial, long nunits, long ncsize,
-                                  double *__restrict__ lag)
+// Pass 1 of the lag reduction: unit group g of cell d sums partial[u][d] for
+// u in [g·U/G, (g+1)·U/G) with a TwoSum-compensated accumulator, in order, and
+// leaves (sum, compensation) in part[g][d] / part[G + g][d].
+__global__ void lag_reduce_groups(const double *__restrict__ partial, long nunits, long ncsize,
+                                  double *__restrict__ part)
 {
-    long d = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long d = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int g = blockIdx.y, G = gridDim.y;
     if (d >= ncsize) return;
+    const long u0 = nunits * g / G, u1 = nunits * (g + 1) / G;
     double s = 0.0, comp = 0.0;
-    for (long u = 0; u < nunits; ++u) {
-        double v = partial[u * ncsize + d];
-        double t = s + v;
-        double bp = t - s;
+    for (long u = u0; u < u1; ++u) {
+        const double v = partial[u * ncsize + d];
+        const double t = s + v;
+        const double bp = t - s;
         comp += (s - (t - bp)) + (v - bp);
         s = t;
+    }
+    part[(long)g * ncsize + d] = s;
+    part[(long)(G + g) * ncsize + d] = comp;
+}
+
+// Pass 2: lag[d] = the groups' sums added in group order (TwoSum again) plus all compensations.
+__global__ void lag_reduce_final(const double *__restrict__ part, int G, long ncsize, double *__restrict__ lag)
+{
+    const long d = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (d >= ncsize) return;
+    double s = 0.0, comp = 0.0;
+    for (int g = 0; g < G; ++g) {
+        const double v = part[(long)g * ncsize + d];
+        const double t = s + v;
+        const double bp = t - s;
+        comp += (s - (t - bp)) + (v - bp);
+        s = t;
+        comp += part[(long)(G + g) * ncsize + d];
     }
     lag[d] = s + comp;
 }
@@ -183,11 +205,19 @@ __global__ void sum_fixed(const double *__restrict__ part, int n, double *__rest
 
 int lag_reduce(amber_cuda_ctx *c, const double *partial, long nunits, long ncsize, double *lag)
 {
+    // enough unit groups to give every SM several blocks; the grouping depends only on
+    // (nunits, ncsize, SM count), so the result is deterministic
+    const long bx = (ncsize + 255) / 256;
+    const long G = std::max<long>(1, std::min<long>({64L, (8L * c->num_sms + bx - 1) / bx, (nunits + 3) / 4}));
+    int rc = ensure(c, c->lagred, sizeof(double) * 2 * (size_t)G * ncsize, "lag reduction scratch");
+    if (rc) return rc;
+    double *part = (double *)c->lagred.p;
     phase_begin(c, 2);
-    lag_reduce_kernel<<<(unsigned)((ncsize + 255) / 256), 256, 0, c->stream>>>(partial, nunits, ncsize, lag);
+    lag_reduce_groups<<<dim3((unsigned)bx, (unsigned)G), 256, 0, c->stream>>>(partial, nunits, ncsize, part);
+    lag_reduce_final<<<(unsigned)bx, 256, 0, c->stream>>>(part, (int)G, ncsize, lag);
     phase_end(c);
-    c->launches += 1;
-    return cuda_check(c, cudaGetLastError(), "lag_reduce_kernel launch");
+    c->launches += 2;
+    return cuda_check(c, cudaGetLastError(), "lag reduction launch");
 }
 
 int contract_fp64(amber_cuda_ctx *c, const double *m1, const double *m2, const double *m3, long k, long kp,
