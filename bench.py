@@ -52,6 +52,12 @@ WORKLOAD = dict(workload="single realisation: 256^2 grid, 128 channels (4 of eve
                 grid=256, channels=128, bins=16, nc10=63, du=0.5, version=2)
 
 
+# DRAM bytes per lag-triple product of contract_i8_kernel, from one ncu capture of a full launch
+# (triangle rp=140 of the single-realisation workload: 227.51 MB for 810152 * 125316 products).
+# Every map row is read once per launch, so traffic grows with products.
+DRAM_BYTES_PER_PRODUCT = 227.51e6 / (810152 * 125316)
+
+
 def peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -326,9 +332,14 @@ def main():
     avg_launch_ms = contract_ms / max(contracts, 1)
     achieved = 2.0 * per_launch_products / (avg_launch_ms * 1e-3) / 1e12
     peak = pk.get("bf16_tflops_sustained", pk.get("bf16_tflops"))
+    # the digit scheme runs 9 int8 MACs per lag-triple product (3 x 4 digits, classes i+j <= 3)
+    int8_tops = 2.0 * 9 * per_launch_products / (avg_launch_ms * 1e-3) / 1e12
     roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-            "traffic": None, "kernel": "contract_i8_kernel",
+            "traffic": DRAM_BYTES_PER_PRODUCT * per_launch_products, "kernel": "contract_i8_kernel",
+            "traffic_source": "ncu dram__bytes_read+write of one launch (profiles/"
+                              "contract_i8_kernel_config2_one_triangle.txt), scaled by products per launch",
             "peak_kind": f"{pk_kind} bf16 dense, sustained (int8 MMA nominal rate is 2x this)",
+            "int8_digit_mmas": {"macs_per_product": 9, "tops": int8_tops, "frac_of_2x_bf16_peak": int8_tops / (2 * peak)},
             "per_launch_products": per_launch_products, "avg_launch_ms": avg_launch_ms,
             "share_of_step": contract_ms / max(sum(step_ms), 1e-9),
             "phase_ms_per_step": {"maps": maps_ms / args.steps, "contract": contract_ms / args.steps,

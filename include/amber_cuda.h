@@ -39,7 +39,7 @@ extern "C" {
 
 /* ---- precision of the triple-product contraction ---- */
 #define AMBER_PREC_FP64 0   /* plain FP64 restatement of the reference loop (CUDA cores) */
-#define AMBER_PREC_MIXED 1  /* int8 tensor cores: 3-digit fixed point, exact int32 accumulation in TMEM,
+#define AMBER_PREC_MIXED 1  /* int8 tensor cores: base-254 fixed-point digits, exact int32 accumulation in TMEM,
                                FP64 recombination and compensated lag reduction (≤1e-6 of Σ|products|) */
 #define AMBER_PREC_BF16X3 2 /* split-BF16×3 on the tensor cores with FP32 accumulation in TMEM; kept for
                                comparison: it misses 1e-6 on coherent v2 sampling-mask sums */
