@@ -256,8 +256,10 @@ void amber_cuda_destroy(amber_cuda_ctx *c)
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);
     DevBuf *bufs[] = {&c->grid, &c->mask, &c->d_weight, &c->d_anchors, &c->y, &c->maps_d, &c->maps_i,
-                      &c->partial, &c->results, &c->ring_lohi, &c->misc, &c->mixed_scratch, &c->lagred};
+                      &c->partial, &c->results, &c->ring_lohi, &c->misc, &c->mixed_scratch, &c->lagred, &c->jobdesc};
     for (DevBuf *b : bufs) release(c, *b);
+    if (c->stage) cudaFreeHost(c->stage);
+    c->stage = nullptr;
     for (auto &kv : c->twiddles) release(c, kv.second);
     for (auto &e : c->phase_ev) {
         cudaEventDestroy(e.a);
@@ -565,6 +567,7 @@ int amber_cuda_triangles_run(amber_cuda_ctx *c, int ntri, const int *tri, int wa
                 phase_end(c);
                 if (rc) return rc;
             }
+            std::vector<I8Job> jobs;  // mixed path: the whole batch goes to the persistent kernel at once
             for (int t : batch) {
                 const size_t s1 = ms.slot_of_ring[tri[3 * t]], s2 = ms.slot_of_ring[tri[3 * t + 1]],
                              s3 = ms.slot_of_ring[tri[3 * t + 2]];
@@ -583,7 +586,16 @@ int amber_cuda_triangles_run(amber_cuda_ctx *c, int ntri, const int *tri, int wa
                             d.expo = b.expo + s * c->nc;
                             return d;
                         };
-                        rc = contract_i8(c, slot(s1), slot(s2), slot(s3), k, kp, lag);
+                        I8Job jb;
+                        jb.m1 = slot(s1); jb.m2 = slot(s2); jb.m3 = slot(s3);
+                        jb.k = k; jb.kp = kp;
+                        jb.nc = (int)c->nc; jb.nc10 = c->nc10;
+                        jb.anchors = (const int *)c->d_anchors.p;
+                        jb.weight = (const int *)c->d_weight.p;
+                        jb.nanchors = (int)c->anchors.size();
+                        jb.lag_out = lag;
+                        jobs.push_back(jb);
+                        rc = AMBER_OK;
                     } else if (prec == AMBER_PREC_BF16X3) {
                         const uint16_t *hi = (const uint16_t *)base;
                         const uint16_t *lo = hi + nvals;
@@ -597,6 +609,7 @@ int amber_cuda_triangles_run(amber_cuda_ctx *c, int ntri, const int *tri, int wa
                 }
                 c->last_products += (double)c->total_vcp * (double)k * (want_v2 ? 2.0 : 1.0);
             }
+            if (!jobs.empty() && (rc = contract_i8_jobs(c, jobs))) return rc;
         }
     }
     cudaEventRecord(c->ev1, c->stream);

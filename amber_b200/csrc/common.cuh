@@ -76,6 +76,9 @@ struct amber_cuda_ctx {
     amber::DevBuf misc;
     amber::DevBuf mixed_scratch;
     amber::DevBuf lagred;  // two-pass lag reduction: per-group sums and compensations
+    amber::DevBuf jobdesc; // contraction job descriptors and work items
+    void *stage = nullptr; // pinned host staging of the job descriptors
+    size_t stage_bytes = 0;
 
     // per-phase device timing of the last run (CUDA events on the launch stream)
     struct PhaseEv {
@@ -136,7 +139,7 @@ int contract_fp64(amber_cuda_ctx *c, const double *m1, const double *m2, const d
 // Split-BF16×3 contraction (tcgen05, FP32 accumulation in TMEM).
 int contract_bf16x3(amber_cuda_ctx *c, const uint16_t *h1, const uint16_t *l1, const uint16_t *h2,
                     const uint16_t *l2, const uint16_t *h3, const uint16_t *l3, long k, long kp, double *lag_out);
-// Mixed-precision contraction: 3-digit int8 fixed point on the tensor cores
+// Mixed-precision contraction: base-254 int8 digits on the tensor cores
 // (tcgen05 kind::i8, exact int32 accumulation in TMEM).
 struct DigitMaps {
     const float *f32;                 // [nc][kp]
@@ -145,6 +148,19 @@ struct DigitMaps {
 };
 int contract_i8(amber_cuda_ctx *c, const DigitMaps &m1, const DigitMaps &m2, const DigitMaps &m3, long k, long kp,
                 double *lag_out);
+// One mixed-precision contraction job: one triangle's D or mask pass of one realisation.
+struct I8Job {
+    DigitMaps m1, m2, m3;   // ring maps of r1, r2, r3 on the job's Ng1 grid
+    long k, kp;             // pixels, row stride
+    int nc, nc10;           // the realisation's channel count and lag half-width
+    const int *anchors;     // device: channels with weight > 0
+    const int *weight;      // device: channel multiplicities
+    int nanchors;
+    double *lag_out;        // device: FP64 lag array [nclen²]
+};
+// All jobs in as few persistent launches as the partial-tile memory allows (jobs of
+// different realisations may share a launch); each job's result depends on the job only.
+int contract_i8_jobs(amber_cuda_ctx *c, const std::vector<I8Job> &jobs);
 // lag[d] = Σ_u partial[u][d] (compensated, fixed order).
 int lag_reduce(amber_cuda_ctx *c, const double *partial, long nunits, long ncsize, double *lag);
 // Σ_x a·b·c over n points (FP64, deterministic) into out[0].

@@ -89,16 +89,26 @@ constexpr int NBI = 2;            // fp32 input stages (D3 tile + D1 row)
 constexpr int NDB = 4;            // int8 digits of the per-anchor product (B)
 constexpr int A_BOX = KB_A * BM;  // one digit plane of one D2 tile: 128 rows × 64 bytes, 64B-swizzled
 
-struct ParamsI8 {
+// One contraction job (one triangle's D or mask pass) as the kernel sees it.
+// Lives in device memory; the tensor maps are read from there by TMA.
+struct alignas(64) JobDesc {
+    CUtensorMap ta[3];  // D2 digit planes: box {64 px, 128 rows}, 64B swizzle
+    CUtensorMap td3;    // D3 fp32: box {32 px, BN rows}, 128B swizzle
+    CUtensorMap td1;    // D1 fp32: box {128 px, 1 row}
     const int *e1, *e2, *e3;  // row exponents [nc]
+    const int *anchors;       // channels with weight > 0
+    const int *weight;        // channel multiplicities [nc]
+    double *partial;          // [anchor][chunk][nclen²]
     long k, kp;
+    long chunk;               // pixels per chunk (multiple of KB_B)
     int nc, nc10, nclen;
     int mt_count, nt_count, nchunk, nanchors;
-    long chunk;  // pixels per chunk (multiple of KB_B)
-    const int *anchors;
-    const int *weight;
-    double *partial;  // [anchor][chunk][nclen²]
-    int *err;
+};
+
+// Work item: job index and the item's index inside the job (chunk-major).
+struct Item {
+    int job;
+    int local;
 };
 
 // Four base-254 digits of two products u·v at once (packed FP32x2): every
@@ -178,11 +188,45 @@ __device__ __forceinline__ void issue_stage(uint32_t tmem, uint32_t a_stage, uin
 
 __device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
+// Decoded work item: everything a role needs to run one (anchor, tile, chunk).
+struct ItemView {
+    const JobDesc *j;
+    int nt, mt, aidx, chunk, p1, nb, bbase, rbase, E1;
+    long x_begin;
+};
+
+template <int BN>
+__device__ __forceinline__ ItemView decode(const JobDesc *jobs, const Item *items, int g)
+{
+    ItemView v;
+    const Item it = items[g];
+    v.j = jobs + it.job;
+    const JobDesc &j = *v.j;
+    long q = it.local;
+    v.nt = (int)(q % j.nt_count);
+    q /= j.nt_count;
+    v.mt = (int)(q % j.mt_count);
+    q /= j.mt_count;
+    v.aidx = (int)(q % j.nanchors);
+    v.chunk = (int)(q / j.nanchors);
+    v.p1 = j.anchors[v.aidx];
+    v.x_begin = (long)v.chunk * j.chunk;
+    const long x_end = min(j.k, v.x_begin + j.chunk);
+    v.nb = (int)((x_end - v.x_begin + KB_B - 1) / KB_B);  // 128-pixel stages
+    v.bbase = v.p1 - j.nc10 + v.nt * BN;                 // first p3 row of the B tile
+    v.rbase = v.p1 - j.nc10 + v.mt * BM;                 // first p2 row of the A tile
+    v.E1 = j.e1[v.p1];
+    return v;
+}
+
+// Persistent: CTA b runs items b, b + gridDim.x, ... of the list (jobs one after the other,
+// each chunk-major, so the CTAs resident at one time share a pixel chunk of one job in L2).
+// The pipelines run on across items: stage and tile counters are global to the CTA, TMEM
+// stays allocated, and the accumulators are handed from the MMA issuers to the epilogue
+// warps and back once per item (acc_full / acc_empty).
 template <int BN>
 __global__ void __launch_bounds__(NTHREADS, 1)
-    contract_i8_kernel(const __grid_constant__ CUtensorMap tm_a0, const __grid_constant__ CUtensorMap tm_a1,
-                       const __grid_constant__ CUtensorMap tm_a2, const __grid_constant__ CUtensorMap tm_d3,
-                       const __grid_constant__ CUtensorMap tm_d1, const ParamsI8 prm)
+    contract_i8_kernel(const JobDesc *__restrict__ jobs, const Item *__restrict__ items, int nitems, int *err)
 {
     constexpr int STAGE_BI = BN * KB_B * 4;         // four 32-pixel fp32 boxes of BN rows (the D1 rows sit apart)
     constexpr int TILE = BN * KB_B;                 // one B digit tile (BN rows × 128 bytes)
@@ -196,44 +240,27 @@ __global__ void __launch_bounds__(NTHREADS, 1)
 
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char *smem = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-    unsigned char *bin = smem;                       // NBI × STAGE_BI
-    unsigned char *bdig = smem + NBI * STAGE_BI;     // NSTAGE × STAGE_BD
+    unsigned char *bin = smem;                        // NBI × STAGE_BI
+    unsigned char *bdig = smem + NBI * STAGE_BI;      // NSTAGE × STAGE_BD
     unsigned char *atile = bdig + NSTAGE * STAGE_BD;  // NAS × 3 × A_BOX
     float *d1rows = reinterpret_cast<float *>(atile + NAS * 3 * A_BOX);  // NBI × KB_B fp32: the D1 row of each input stage
     uint64_t *bars = reinterpret_cast<uint64_t *>(d1rows + NBI * KB_B);
     uint64_t *as_full = bars, *as_empty = as_full + NAS;
     uint64_t *bin_full = as_empty + NAS, *bin_empty = bin_full + NBI;
     uint64_t *st_full = bin_empty + NBI, *st_empty = st_full + NSTAGE;
-    uint64_t *acc_full = st_empty + NSTAGE;
-    uint64_t *drain = acc_full + 1;  // one per issuer
+    uint64_t *acc_full = st_empty + NSTAGE, *acc_empty = acc_full + 1;
+    uint64_t *drain = acc_empty + 1;  // one per issuer
     volatile uint32_t *tmem_slot = reinterpret_cast<volatile uint32_t *>(drain + NISSUE);
     volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-
-    // Chunk-major order: the CTAs resident at one time share a pixel chunk, so
-    // that chunk of every map row stays in L2 while all anchors read it.
-    long item = blockIdx.x;
-    const int nt = (int)(item % prm.nt_count);
-    item /= prm.nt_count;
-    const int mt = (int)(item % prm.mt_count);
-    item /= prm.mt_count;
-    const int aidx = (int)(item % prm.nanchors);
-    const int chunk = (int)(item / prm.nanchors);
-    const int p1 = prm.anchors[aidx];
-    const long x_begin = (long)chunk * prm.chunk;
-    const long x_end = min(prm.k, x_begin + prm.chunk);
-    const int nb = (int)((x_end - x_begin + KB_B - 1) / KB_B);  // 128-pixel stages
-    const int na = 2 * nb;                                      // 64-pixel D2 tiles
-    const int bbase = p1 - prm.nc10 + nt * BN;                  // first p3 row of the B tile
-    const int rbase = p1 - prm.nc10 + mt * BM;                  // first p2 row of the A tile
-    const int E1 = prm.e1[p1];
 
     if (tid == 0) {
         for (int s = 0; s < NAS; ++s) { mbar_init(&as_full[s], 1); mbar_init(&as_empty[s], NWARP_A); }
         for (int s = 0; s < NBI; ++s) { mbar_init(&bin_full[s], 1); mbar_init(&bin_empty[s], NWARP_B); }
         for (int s = 0; s < NSTAGE; ++s) { mbar_init(&st_full[s], NWARP_A + NWARP_B); mbar_init(&st_empty[s], NISSUE); }
         mbar_init(acc_full, NISSUE);
+        mbar_init(acc_empty, NEPI);
         for (int q = 0; q < NISSUE; ++q) mbar_init(&drain[q], 1);
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -254,45 +281,52 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         // fp32 inputs of the B formers: D3 rows [bbase, bbase+BN) as four 32-pixel swizzled boxes, D1 row p1.
         // Pixels past the end of the map and rows outside [0, nc) come back as zeros.
         if (lane == 0) {
-            int issued = 0;
-            for (int it = 0; it < nb; ++it) {
-                const int s = it % NBI;
-                if (!mbar_wait(&bin_empty[s], ((it / NBI) & 1) ^ 1, abort_flag, prm.err, 1)) break;
-                unsigned char *t = bin + s * STAGE_BI;
-                mbar_expect_tx(&bin_full[s], BN * KB_B * 4 + KB_B * 4);
-                const int x = (int)(x_begin + (long)it * KB_B);
+            int gs = 0;  // stages issued so far
+            for (int g = blockIdx.x; g < nitems && ok; g += gridDim.x) {
+                const ItemView v = decode<BN>(jobs, items, g);
+                for (int it = 0; it < v.nb; ++it, ++gs) {
+                    const int s = (gs % NBI);
+                    if (!mbar_wait(&bin_empty[s], ((gs / NBI) & 1) ^ 1, abort_flag, err, 1)) { ok = false; break; }
+                    unsigned char *t = bin + s * STAGE_BI;
+                    mbar_expect_tx(&bin_full[s], BN * KB_B * 4 + KB_B * 4);
+                    const int x = (int)(v.x_begin + (long)it * KB_B);
 #pragma unroll
-                for (int j = 0; j < 4; ++j) tma_load_2d(t + j * (BN * 128), &tm_d3, &bin_full[s], x + 32 * j, bbase);
-                tma_load_2d(d1rows + s * KB_B, &tm_d1, &bin_full[s], x, p1);
-                ++issued;
+                    for (int jb = 0; jb < 4; ++jb)
+                        tma_load_2d(t + jb * (BN * 128), &v.j->td3, &bin_full[s], x + 32 * jb, v.bbase);
+                    tma_load_2d(d1rows + s * KB_B, &v.j->td1, &bin_full[s], x, v.p1);
+                }
             }
-            if (*abort_flag)
-                for (int it = max(0, issued - NBI); it < issued; ++it)
-                    for (long long i = 0; i < WAIT_LIMIT && !mbar_try_wait(&bin_full[it % NBI], (it / NBI) & 1); ++i)
+            if (!ok)
+                for (int q = max(0, gs - NBI); q < gs; ++q)
+                    for (long long i = 0; i < WAIT_LIMIT && !mbar_try_wait(&bin_full[q % NBI], ((q / NBI) & 1)); ++i)
                         __nanosleep(100);
         }
     } else if (warp == WARP_TMA_A) {
         // D2 digit planes, rows [rbase, rbase+128) × 64 pixels per tile; rows outside [0, nc) and
         // pixels past the end of the map come back as zeros.
         if (lane == 0) {
-            int issued = 0;
-            for (int ia = 0; ia < na; ++ia) {
-                const int s = ia % NAS;
-                if (!mbar_wait(&as_empty[s], ((ia / NAS) & 1) ^ 1, abort_flag, prm.err, 8)) break;
-                unsigned char *t = atile + s * 3 * A_BOX;
-                mbar_expect_tx(&as_full[s], 3 * A_BOX);
-                const int x = (int)(x_begin + (long)ia * KB_A);
-                tma_load_2d(t, &tm_a0, &as_full[s], x, rbase);
-                tma_load_2d(t + A_BOX, &tm_a1, &as_full[s], x, rbase);
-                tma_load_2d(t + 2 * A_BOX, &tm_a2, &as_full[s], x, rbase);
-                ++issued;
+            int gt = 0;  // tiles issued so far
+            for (int g = blockIdx.x; g < nitems && ok; g += gridDim.x) {
+                const ItemView v = decode<BN>(jobs, items, g);
+                for (int ia = 0; ia < 2 * v.nb; ++ia, ++gt) {
+                    const int s = (gt % NAS);
+                    if (!mbar_wait(&as_empty[s], ((gt / NAS) & 1) ^ 1, abort_flag, err, 8)) { ok = false; break; }
+                    unsigned char *t = atile + s * 3 * A_BOX;
+                    mbar_expect_tx(&as_full[s], 3 * A_BOX);
+                    const int x = (int)(v.x_begin + (long)ia * KB_A);
+                    tma_load_2d(t, &v.j->ta[0], &as_full[s], x, v.rbase);
+                    tma_load_2d(t + A_BOX, &v.j->ta[1], &as_full[s], x, v.rbase);
+                    tma_load_2d(t + 2 * A_BOX, &v.j->ta[2], &as_full[s], x, v.rbase);
+                }
             }
-            if (*abort_flag)
-                for (int ia = max(0, issued - NAS); ia < issued; ++ia)
-                    for (long long i = 0; i < WAIT_LIMIT && !mbar_try_wait(&as_full[ia % NAS], (ia / NAS) & 1); ++i)
+            if (!ok)
+                for (int q = max(0, gt - NAS); q < gt; ++q)
+                    for (long long i = 0; i < WAIT_LIMIT && !mbar_try_wait(&as_full[q % NAS], ((q / NAS) & 1)); ++i)
                         __nanosleep(100);
         }
     } else if (warp == WARP_MMA || warp == WARP_MMA2) {
+        // Two issuers feed the tensor pipe from independent instruction streams, so one
+        // thread's barrier wait or commit does not leave the pipe idle.
         if (lane == 0) {
             const int q = warp == WARP_MMA ? 0 : 1;
             // S32 accumulate, signed int8 A and B, both K-major, M = 128, N = BN
@@ -300,152 +334,171 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                                    ((uint32_t)(BM >> 4) << 24);
             // descriptors are linear in the start address (bits 0-13, 16-byte units)
             const uint64_t desc0 = smem_desc_sw128(smem_u32(bdig));
-            for (int it = 0; it < nb; ++it) {
-                const int s = it & 1;
-                if (!mbar_wait(&st_full[s], (it >> 1) & 1, abort_flag, prm.err, 2)) { ok = false; break; }
-                fence_after();
-                issue_stage<BN>(tmem, tmem + A_COL0 + s * A_STAGE_COLS, desc0 + (uint64_t)((s * STAGE_BD) >> 4), idesc,
-                                q, it == 0);
-                umma_commit(&st_empty[s]);
+            int gs = 0, seq = 0;
+            for (int g = blockIdx.x; g < nitems && ok; g += gridDim.x, ++seq) {
+                const int nb = decode<BN>(jobs, items, g).nb;
+                // the epilogue of the previous item has read the accumulators out
+                if (!mbar_wait(acc_empty, (seq & 1) ^ 1, abort_flag, err, 10)) { ok = false; break; }
+                for (int it = 0; it < nb; ++it, ++gs) {
+                    const int s = (gs & 1);
+                    if (!mbar_wait(&st_full[s], ((gs >> 1) & 1), abort_flag, err, 2)) { ok = false; break; }
+                    fence_after();
+                    issue_stage<BN>(tmem, tmem + A_COL0 + s * A_STAGE_COLS, desc0 + (uint64_t)((s * STAGE_BD) >> 4),
+                                    idesc, q, it == 0);
+                    umma_commit(&st_empty[s]);
+                }
+                if (ok) umma_commit(acc_full);
             }
-            if (ok) {
-                umma_commit(acc_full);
-            } else {
+            if (!ok) {
                 umma_commit(&drain[q]);
                 for (long long i = 0; i < WAIT_LIMIT && !mbar_try_wait(&drain[q], 0); ++i) __nanosleep(100);
             }
         }
-    } else if (warp < NWARP_A) {
-        // ---- D2 digits → TMEM: warp w moves TMEM lanes [32w, 32w+32), all 64 pixels of each tile ----
-        // Row m of a 64B-swizzled box holds its 16-byte chunk c at position c ^ ((m >> 1) & 3), so
-        // eight consecutive rows reading the same chunk hit eight different bank groups.
-        // tcgen05.st reads its source registers asynchronously: they are not reused before
-        // tcgen05.wait::st, and a tile's shared memory is released only after that wait.
+    } else {
+        // ---- warps 0-19: D2 movers (0-3) and B formers (4-19); warps 0-15 also run each item's epilogue ----
+        const bool mover = warp < NWARP_A;
+        // mover: TMEM lanes [32w, 32w+32), all 64 pixels of each tile
         const int m = (warp << 5) + lane;
-        const uint32_t lane_field = (uint32_t)(warp << 5) << 16;
+        const uint32_t lane_field = (uint32_t)((warp & 3) << 5) << 16;
         const int sw = (m >> 1) & 3;
-        for (int it = 0; it < nb && ok; ++it) {
-            const int s = it & 1;
-#pragma unroll 1
-            for (int h = 0; h < 2; ++h) {
-                const int ia = 2 * it + h, sa = ia % NAS;
-                if (!mbar_wait_warp(&as_full[sa], (ia / NAS) & 1, abort_flag, prm.err, 9)) { ok = false; break; }
-                const unsigned char *t = atile + sa * 3 * A_BOX + m * KB_A;
-                uint32_t v[3][16];
-#pragma unroll
-                for (int d = 0; d < 3; ++d)
-#pragma unroll
-                    for (int c = 0; c < 4; ++c) {
-                        const uint4 x = *reinterpret_cast<const uint4 *>(t + d * A_BOX + ((c ^ sw) << 4));
-                        v[d][4 * c] = x.x; v[d][4 * c + 1] = x.y; v[d][4 * c + 2] = x.z; v[d][4 * c + 3] = x.w;
-                    }
-                if (h == 0) {
-                    if (!mbar_wait_warp(&st_empty[s], ((it >> 1) & 1) ^ 1, abort_flag, prm.err, 4)) { ok = false; break; }
-                    fence_after();
-                }
-                // pixels 64h .. 64h+63 of the stage = 32-pixel slices 2h, 2h+1: columns 16h .. 16h+15 of each digit
-                const uint32_t col = tmem + lane_field + A_COL0 + s * A_STAGE_COLS + 16 * h;
-#pragma unroll
-                for (int d = 0; d < 3; ++d) tmem_st16(col + 32 * d, v[d]);
-                asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
-                __syncwarp();
-                if (lane == 0) mbar_arrive(&as_empty[sa]);
-            }
-            if (!ok) break;
-            fence_before();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&st_full[s]);
-        }
-    } else if (warp < NWARP_A + NWARP_B) {
-        // ---- B formers: thread (row n, segment sg) forms PT pixels of D1[p1]·D3[bbase+n] per stage ----
-        const int tb = tid - NWARP_A * 32;  // 0 .. 32·NWARP_B − 1
+        // former: thread (row n, segment sg) forms PT pixels of D1[p1]·D3[bbase+n] per stage
+        const int tb = tid - NWARP_A * 32;
         const int n = tb % BN, sg = tb / BN;
-        const int px0 = sg * PT;  // first pixel of this thread inside the 128-pixel stage
-        const int p3 = bbase + n;
-        const bool col_ok = p3 >= 0 && p3 < prm.nc;
-        const float scale = col_ok ? ldexpf(127.f, -(E1 + prm.e3[p3])) : 0.f;
-        const float2 sc2 = make_float2(scale, scale);
+        const int px0 = sg * PT;
         const int box = px0 / 32, c0 = (px0 % 32) / 4;  // input box and first 16-byte chunk in it
         // destination: 16-byte chunk px0/16 of each 128-byte digit row, at its swizzled position; PT = 8
         // fills one half of it
         const int dst_off = n * 128 + (((px0 / 16) ^ (n & 7)) << 4) + (px0 % 16);
-        for (int it = 0; it < nb; ++it) {
-            const int si = it % NBI, s = it & 1;
-            if (!mbar_wait_warp(&bin_full[si], (it / NBI) & 1, abort_flag, prm.err, 6)) { ok = false; break; }
-            const unsigned char *rowp = bin + si * STAGE_BI + box * (BN * 128) + n * 128;
-            const float *d1p = d1rows + si * KB_B + px0;
-            uint32_t w[NDB][PT / 4];
-#pragma unroll
-            for (int q = 0; q < PT / 4; ++q) {
-                const float4 v = *reinterpret_cast<const float4 *>(rowp + (((c0 + q) ^ (n & 7)) << 4));
-                const float4 u = *reinterpret_cast<const float4 *>(d1p + 4 * q);
-                float2 ya0, ya1, ya2, ya3, yb0, yb1, yb2, yb3;
-                digits254x2(__fmul2_rn(make_float2(u.x, u.y), sc2), make_float2(v.x, v.y), ya0, ya1, ya2, ya3);
-                digits254x2(__fmul2_rn(make_float2(u.z, u.w), sc2), make_float2(v.z, v.w), yb0, yb1, yb2, yb3);
-                w[0][q] = pack_low_bytes(ya0.x, ya0.y, yb0.x, yb0.y);
-                w[1][q] = pack_low_bytes(ya1.x, ya1.y, yb1.x, yb1.y);
-                w[2][q] = pack_low_bytes(ya2.x, ya2.y, yb2.x, yb2.y);
-                w[3][q] = pack_low_bytes(ya3.x, ya3.y, yb3.x, yb3.y);
-            }
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&bin_empty[si]);
-            if (!mbar_wait_warp(&st_empty[s], ((it >> 1) & 1) ^ 1, abort_flag, prm.err, 7)) { ok = false; break; }
-            unsigned char *dst = bdig + s * STAGE_BD + dst_off;
-#pragma unroll
-            for (int d = 0; d < NDB; ++d) {
-                if constexpr (PT == 16)
-                    *reinterpret_cast<uint4 *>(dst + d * TILE) = make_uint4(w[d][0], w[d][1], w[d][2], w[d][3]);
-                else
-                    *reinterpret_cast<uint2 *>(dst + d * TILE) = make_uint2(w[d][0], w[d][1]);
-            }
-            fence_proxy_async_smem();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&st_full[s]);
-        }
-    }
-
-    // ---- epilogue (warps 0-15): int32 digit accumulators → FP64 partial tile; warpgroup wg reads BN/4 columns ----
-    if (warp < NEPI) {
-        const int wg = warp >> 2;
-        const int m = ((warp & 3) << 5) + lane;
-        const uint32_t lane_field = (uint32_t)((warp & 3) << 5) << 16;
-        const bool good = __all_sync(0xffffffffu, ok) && mbar_wait_warp(acc_full, 0, abort_flag, prm.err, 5);
-        if (good) {
+        int gs = 0, gt = 0, seq = 0;
+        // ---- epilogue (warps 0-15): int32 digit accumulators → FP64 partial tile; warpgroup wg reads BN/4 columns ----
+        auto epilogue_item = [&](int g) {
+            const ItemView v = decode<BN>(jobs, items, g);
+            const JobDesc &j = *v.j;
+            const int wg = warp >> 2;
+            const int me = ((warp & 3) << 5) + lane;
+            const bool good = __all_sync(0xffffffffu, ok) && mbar_wait_warp(acc_full, (seq & 1), abort_flag, err, 5);
+            if (!good) { ok = false; return; }
             fence_after();
-            const int d2 = mt * BM + m;
-            const int p2 = rbase + m;
-            const bool row_ok = d2 < prm.nclen && p2 >= 0 && p2 < prm.nc && prm.weight[p2] > 0;
-            const int E12 = E1 + (row_ok ? prm.e2[p2] : 0);
-            const double wr = row_ok ? (double)prm.weight[p1] * (double)prm.weight[p2] : 0.0;
+            const int d2 = v.mt * BM + me;
+            const int p2 = v.rbase + me;
+            const bool row_ok = d2 < j.nclen && p2 >= 0 && p2 < j.nc && j.weight[p2] > 0;
+            const int E12 = v.E1 + (row_ok ? j.e2[p2] : 0);
+            const double wr = row_ok ? (double)j.weight[v.p1] * (double)j.weight[p2] : 0.0;
             double *dst = nullptr;
-            if (d2 < prm.nclen)
-                dst = prm.partial + ((long)aidx * prm.nchunk + chunk) * prm.nclen * prm.nclen + (long)d2 * prm.nclen;
+            if (d2 < j.nclen)
+                dst = j.partial + ((long)v.aidx * j.nchunk + v.chunk) * j.nclen * j.nclen + (long)d2 * j.nclen;
             const int c_begin = wg * (BN / 4), c_end = c_begin + BN / 4;
             const double i254 = 1.0 / 254.0, i254_2 = i254 * i254, i254_3 = i254_2 * i254;
-            for (int c0 = c_begin; c0 < c_end; c0 += 8) {
+            for (int cb = c_begin; cb < c_end; cb += 8) {
                 uint32_t v0[8], v1[8], v2[8], v3[8];
-                tmem_ld8(tmem + lane_field + c0, v0);
-                tmem_ld8(tmem + lane_field + BN + c0, v1);
-                tmem_ld8(tmem + lane_field + 2 * BN + c0, v2);
-                tmem_ld8(tmem + lane_field + 3 * BN + c0, v3);
+                tmem_ld8(tmem + lane_field + cb, v0);
+                tmem_ld8(tmem + lane_field + BN + cb, v1);
+                tmem_ld8(tmem + lane_field + 2 * BN + cb, v2);
+                tmem_ld8(tmem + lane_field + 3 * BN + cb, v3);
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                if (cb + 8 >= c_end) {
+                    // last read of this item: hand the accumulators back to the MMA issuers
+                    fence_before();
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(acc_empty);
+                }
                 if (dst) {
 #pragma unroll
-                    for (int j = 0; j < 8; ++j) {
-                        const int nn = c0 + j;
-                        const int d3 = nt * BN + nn;
-                        if (d3 >= prm.nclen) continue;
-                        const int p3 = bbase + nn;
+                    for (int e = 0; e < 8; ++e) {
+                        const int nn = cb + e;
+                        const int d3 = v.nt * BN + nn;
+                        if (d3 >= j.nclen) continue;
+                        const int p3 = v.bbase + nn;
                         double val = 0.0;
-                        if (wr != 0.0 && p3 >= 0 && p3 < prm.nc && prm.weight[p3] > 0) {
-                            const double s = (double)(int)v0[j] + (double)(int)v1[j] * i254 +
-                                             (double)(int)v2[j] * i254_2 + (double)(int)v3[j] * i254_3;
-                            val = ldexp(s * (1.0 / 16129.0), E12 + prm.e3[p3]) * wr * (double)prm.weight[p3];
+                        if (wr != 0.0 && p3 >= 0 && p3 < j.nc && j.weight[p3] > 0) {
+                            const double sm = (double)(int)v0[e] + (double)(int)v1[e] * i254 +
+                                              (double)(int)v2[e] * i254_2 + (double)(int)v3[e] * i254_3;
+                            val = ldexp(sm * (1.0 / 16129.0), E12 + j.e3[p3]) * wr * (double)j.weight[p3];
                         }
                         dst[d3] = val;
                     }
                 }
             }
+        };
+        for (int g = blockIdx.x; g < nitems && ok; g += gridDim.x, ++seq) {
+            const ItemView v = decode<BN>(jobs, items, g);
+            const JobDesc &j = *v.j;
+            if (mover) {
+                // tcgen05.st reads its source registers asynchronously: they are not reused before
+                // tcgen05.wait::st, and a tile's shared memory is released only after that wait.
+                for (int it = 0; it < v.nb && ok; ++it, ++gs) {
+                    const int s = (gs & 1);
+#pragma unroll 1
+                    for (int h = 0; h < 2; ++h, ++gt) {
+                        const int sa = (gt % NAS);
+                        if (!mbar_wait_warp(&as_full[sa], ((gt / NAS) & 1), abort_flag, err, 9)) { ok = false; break; }
+                        const unsigned char *t = atile + sa * 3 * A_BOX + m * KB_A;
+                        uint32_t r[3][16];
+#pragma unroll
+                        for (int d = 0; d < 3; ++d)
+#pragma unroll
+                            for (int c = 0; c < 4; ++c) {
+                                const uint4 x = *reinterpret_cast<const uint4 *>(t + d * A_BOX + ((c ^ sw) << 4));
+                                r[d][4 * c] = x.x; r[d][4 * c + 1] = x.y; r[d][4 * c + 2] = x.z; r[d][4 * c + 3] = x.w;
+                            }
+                        if (h == 0) {
+                            if (!mbar_wait_warp(&st_empty[s], ((gs >> 1) & 1) ^ 1, abort_flag, err, 4)) { ok = false; break; }
+                            fence_after();
+                        }
+                        // pixels 64h .. 64h+63 of the stage = 32-pixel slices 2h, 2h+1: columns 16h .. 16h+15 of each digit
+                        const uint32_t col = tmem + lane_field + A_COL0 + s * A_STAGE_COLS + 16 * h;
+#pragma unroll
+                        for (int d = 0; d < 3; ++d) tmem_st16(col + 32 * d, r[d]);
+                        asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+                        __syncwarp();
+                        if (lane == 0) mbar_arrive(&as_empty[sa]);
+                    }
+                    if (!ok) break;
+                    fence_before();
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(&st_full[s]);
+                }
+            } else {
+                const int p3 = v.bbase + n;
+                const bool col_ok = p3 >= 0 && p3 < j.nc;
+                const float scale = col_ok ? ldexpf(127.f, -(v.E1 + j.e3[p3])) : 0.f;
+                const float2 sc2 = make_float2(scale, scale);
+                for (int it = 0; it < v.nb; ++it, ++gs) {
+                    const int si = (gs % NBI), s = (gs & 1);
+                    if (!mbar_wait_warp(&bin_full[si], ((gs / NBI) & 1), abort_flag, err, 6)) { ok = false; break; }
+                    const unsigned char *rowp = bin + si * STAGE_BI + box * (BN * 128) + n * 128;
+                    const float *d1p = d1rows + si * KB_B + px0;
+                    uint32_t w[NDB][PT / 4];
+#pragma unroll
+                    for (int q = 0; q < PT / 4; ++q) {
+                        const float4 x3 = *reinterpret_cast<const float4 *>(rowp + (((c0 + q) ^ (n & 7)) << 4));
+                        const float4 u = *reinterpret_cast<const float4 *>(d1p + 4 * q);
+                        float2 ya0, ya1, ya2, ya3, yb0, yb1, yb2, yb3;
+                        digits254x2(__fmul2_rn(make_float2(u.x, u.y), sc2), make_float2(x3.x, x3.y), ya0, ya1, ya2, ya3);
+                        digits254x2(__fmul2_rn(make_float2(u.z, u.w), sc2), make_float2(x3.z, x3.w), yb0, yb1, yb2, yb3);
+                        w[0][q] = pack_low_bytes(ya0.x, ya0.y, yb0.x, yb0.y);
+                        w[1][q] = pack_low_bytes(ya1.x, ya1.y, yb1.x, yb1.y);
+                        w[2][q] = pack_low_bytes(ya2.x, ya2.y, yb2.x, yb2.y);
+                        w[3][q] = pack_low_bytes(ya3.x, ya3.y, yb3.x, yb3.y);
+                    }
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(&bin_empty[si]);
+                    if (!mbar_wait_warp(&st_empty[s], ((gs >> 1) & 1) ^ 1, abort_flag, err, 7)) { ok = false; break; }
+                    unsigned char *dst = bdig + s * STAGE_BD + dst_off;
+#pragma unroll
+                    for (int d = 0; d < NDB; ++d) {
+                        if constexpr (PT == 16)
+                            *reinterpret_cast<uint4 *>(dst + d * TILE) = make_uint4(w[d][0], w[d][1], w[d][2], w[d][3]);
+                        else
+                            *reinterpret_cast<uint2 *>(dst + d * TILE) = make_uint2(w[d][0], w[d][1]);
+                    }
+                    fence_proxy_async_smem();
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(&st_full[s]);
+                }
+            }
+            if (warp >= NEPI) continue;
+            epilogue_item(g);
         }
     }
 
@@ -489,31 +542,18 @@ int encode(amber_cuda_ctx *c, CUtensorMap *m, CUtensorMapDataType dt, const void
     return AMBER_OK;
 }
 
-template <int BN>
-int launch(amber_cuda_ctx *c, const CUtensorMap (&ta)[3], const CUtensorMap &td3, const CUtensorMap &td1,
-           const ParamsI8 &prm, long items)
-{
-    const size_t sm = smem_bytes<BN>();
-    cudaFuncSetAttribute(contract_i8_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    phase_begin(c, 1);
-    contract_i8_kernel<BN><<<(unsigned)items, NTHREADS, sm, c->stream>>>(ta[0], ta[1], ta[2], td3, td1, prm);
-    phase_end(c);
-    c->launches += 1;
-    c->contractions += 1;
-    return cuda_check(c, cudaGetLastError(), "contract_i8_kernel launch");
-}
-
-// Pixel chunks per (anchor, tile) pair.  One CTA runs per SM, so the launch
-// takes ceil(items / SMs) rounds of one chunk each; more chunks shorten a
-// round but add a fixed cost per CTA (pipeline fill, epilogue) and partial
-// tiles for lag_reduce to read.  Picks the count with the least modelled time.
+// Pixel chunks per (anchor, tile) pair of one job.  One CTA runs per SM; more chunks give
+// more, shorter items (a shorter tail when this job runs alone) but add a fixed cost per
+// item (pipeline fill, epilogue) and partial tiles for lag_reduce to read.  Picks the count
+// with the least modelled time of the job on its own, so the choice (and with it the FP64
+// summation grouping) depends on the job only, never on what else shares the launch.
 long choose_chunks(long k, long pairs, int sms, long ncsize, long max_chunk)
 {
     const long nch_min = std::max<long>(1, (k + max_chunk - 1) / max_chunk);
     const long nch_max = std::max<long>(nch_min, std::min<long>(4 * nch_min + 16, (k + 1023) / 1024));
-    const double stage_s = 0.65e-6;     // one 128-pixel stage of one CTA
-    const double fixed_s = 6 * stage_s;  // fill, drain and epilogue of one CTA
-    const double reduce_bw = 5e12;      // bytes/s for lag_reduce reading the partial tiles
+    const double stage_s = 0.65e-6;      // one 128-pixel stage of one CTA
+    const double fixed_s = 6 * stage_s;  // fill, drain and epilogue of one item
+    const double reduce_bw = 5e12;       // bytes/s for lag_reduce reading the partial tiles
     long best = nch_min;
     double best_t = 1e300;
     for (long nch = nch_min; nch <= nch_max; ++nch) {
@@ -527,57 +567,173 @@ long choose_chunks(long k, long pairs, int sms, long ncsize, long max_chunk)
     return best;
 }
 
+struct Planned {
+    const I8Job *job;
+    int bn, mt, nt;
+    long nch, chunk;
+    size_t partial_bytes;
+};
+
+template <int BN>
+int launch(amber_cuda_ctx *c, const JobDesc *d_jobs, const Item *d_items, long nitems, long grid_ctas, int *d_err)
+{
+    const size_t sm = smem_bytes<BN>();
+    cudaFuncSetAttribute(contract_i8_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    const unsigned grid = (unsigned)std::min<long>(nitems, grid_ctas);
+    contract_i8_kernel<BN><<<grid, NTHREADS, sm, c->stream>>>(d_jobs, d_items, (int)nitems, d_err);
+    c->launches += 1;
+    c->contractions += 1;
+    return cuda_check(c, cudaGetLastError(), "contract_i8_kernel launch");
+}
+
+// Host side of one launch: descriptors and items written into the pinned staging area.
+struct LaunchPlan {
+    std::vector<Planned> jobs;
+    size_t desc_off = 0, item_off = 0;  // byte offsets in the staging area / device job list
+    long nitems = 0;
+    size_t partial_bytes = 0;
+    bool persistent = true;  // false: one CTA per item, dispatched by the hardware as SMs free up
+};
+
+int fill_launch(amber_cuda_ctx *c, LaunchPlan &lp, char *stage)
+{
+    int rc;
+    const int BN = lp.jobs[0].bn;
+    JobDesc *desc = (JobDesc *)(stage + lp.desc_off);
+    Item *items = (Item *)(stage + lp.item_off);
+    size_t poff = 0;
+    long ni = 0;
+    const CUtensorMapDataType u8 = CU_TENSOR_MAP_DATA_TYPE_UINT8, f32 = CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+    for (size_t i = 0; i < lp.jobs.size(); ++i) {
+        const Planned &p = lp.jobs[i];
+        const I8Job &jb = *p.job;
+        JobDesc &d = desc[i];
+        memset(&d, 0, sizeof(d));
+        const int8_t *planes[3] = {jb.m2.d0, jb.m2.d1, jb.m2.d2};
+        for (int q = 0; q < 3; ++q)
+            if ((rc = encode(c, &d.ta[q], u8, planes[q], jb.k, jb.kp, jb.nc, KB_A, BM, CU_TENSOR_MAP_SWIZZLE_64B)))
+                return rc;
+        if ((rc = encode(c, &d.td3, f32, jb.m3.f32, jb.k, jb.kp * 4, jb.nc, 32, BN, CU_TENSOR_MAP_SWIZZLE_128B)))
+            return rc;
+        if ((rc = encode(c, &d.td1, f32, jb.m1.f32, jb.k, jb.kp * 4, jb.nc, KB_B, 1, CU_TENSOR_MAP_SWIZZLE_NONE)))
+            return rc;
+        d.e1 = jb.m1.expo; d.e2 = jb.m2.expo; d.e3 = jb.m3.expo;
+        d.anchors = jb.anchors;
+        d.weight = jb.weight;
+        d.partial = (double *)((char *)c->partial.p + poff);
+        d.k = jb.k; d.kp = jb.kp; d.chunk = p.chunk;
+        d.nc = jb.nc; d.nc10 = jb.nc10; d.nclen = 2 * jb.nc10 + 1;
+        d.mt_count = p.mt; d.nt_count = p.nt; d.nchunk = (int)p.nch; d.nanchors = jb.nanchors;
+        const long n_local = (long)jb.nanchors * p.mt * p.nt * p.nch;
+        for (long q = 0; q < n_local; ++q) items[ni++] = Item{(int)i, (int)q};
+        poff += p.partial_bytes;
+    }
+    return AMBER_OK;
+}
+
 }  // namespace
 
-int contract_i8(amber_cuda_ctx *c, const DigitMaps &m1, const DigitMaps &m2, const DigitMaps &m3, long k, long kp,
-                double *lag_out)
+int contract_i8_jobs(amber_cuda_ctx *c, const std::vector<I8Job> &jobs)
 {
-    const int nc10 = c->nc10, nclen = 2 * nc10 + 1;
-    const long ncsize = (long)nclen * nclen;
-    const int nA = (int)c->anchors.size();
-    if (nA == 0) return cuda_check(c, cudaMemsetAsync(lag_out, 0, sizeof(double) * ncsize, c->stream), "zero lag");
-    const int MT = (nclen + BM - 1) / BM;
-    const int BN = nclen <= 32 ? 32 : 64;
-    const int NT = (nclen + BN - 1) / BN;
-    const long base_items = (long)nA * MT * NT;
-    long max_chunk = c->chunk_px > 0 ? std::min<long>(c->chunk_px, 32768) : 32768;
-    max_chunk = std::max<long>(KB_B, max_chunk / KB_B * KB_B);
-    long nch = choose_chunks(k, base_items, c->num_sms, ncsize, max_chunk);
-    const long chunk = ((k + nch - 1) / nch + KB_B - 1) / KB_B * KB_B;
-    nch = (k + chunk - 1) / chunk;
-
     int rc;
-    const size_t pbytes = sizeof(double) * (size_t)nA * nch * ncsize;
-    if ((rc = ensure(c, c->partial, pbytes, "partial lag tiles"))) return rc;
     if ((rc = ensure(c, c->misc, 256, "error flag"))) return rc;
     int *d_err = (int *)c->misc.p;
     if ((rc = cuda_check(c, cudaMemsetAsync(d_err, 0, sizeof(int), c->stream), "error flag"))) return rc;
-
-    CUtensorMap ta[3], td3, td1;
-    const CUtensorMapDataType u8 = CU_TENSOR_MAP_DATA_TYPE_UINT8, f32 = CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
-    const int8_t *planes[3] = {m2.d0, m2.d1, m2.d2};
-    for (int d = 0; d < 3; ++d)
-        if ((rc = encode(c, &ta[d], u8, planes[d], k, kp, c->nc, KB_A, BM, CU_TENSOR_MAP_SWIZZLE_64B))) return rc;
-    if ((rc = encode(c, &td3, f32, m3.f32, k, kp * 4, c->nc, 32, BN, CU_TENSOR_MAP_SWIZZLE_128B))) return rc;
-    if ((rc = encode(c, &td1, f32, m1.f32, k, kp * 4, c->nc, KB_B, 1, CU_TENSOR_MAP_SWIZZLE_NONE))) return rc;
-    ParamsI8 prm{};
-    prm.nanchors = nA;
-    prm.e1 = m1.expo; prm.e2 = m2.expo; prm.e3 = m3.expo;
-    prm.k = k; prm.kp = kp;
-    prm.nc = (int)c->nc; prm.nc10 = nc10; prm.nclen = nclen;
-    prm.mt_count = MT; prm.nt_count = NT; prm.nchunk = (int)nch; prm.chunk = chunk;
-    prm.anchors = (const int *)c->d_anchors.p;
-    prm.weight = (const int *)c->d_weight.p;
-    prm.partial = (double *)c->partial.p;
-    prm.err = d_err;
-    const long items = base_items * nch;
-    switch (BN) {
-        case 32: rc = launch<32>(c, ta, td3, td1, prm, items); break;
-        case 64: rc = launch<64>(c, ta, td3, td1, prm, items); break;
-        default: rc = fail(c, AMBER_ERR_ARG, "no int8 tile configuration for nclen=%d (BN=%d)", nclen, BN);
+    long max_chunk = c->chunk_px > 0 ? std::min<long>(c->chunk_px, 32768) : 32768;
+    max_chunk = std::max<long>(KB_B, max_chunk / KB_B * KB_B);
+    // Launch plan.  A job with many items runs in a launch of its own with one CTA per
+    // item: the hardware hands items to SMs as they free up (even with uneven items) and
+    // the resident CTAs stay on one pixel chunk of one job (L2 reuse of the maps).  Small
+    // jobs share persistent launches (one CTA per SM looping over the list), so a batch
+    // of them fills the GPU without a tail per job.  Partial tiles of one launch stay
+    // within a slice of the budget.
+    const size_t pcap = std::max<size_t>((size_t)512 << 20, std::min<size_t>((size_t)8 << 30, c->budget / 8));
+    const long big_items = 4L * c->num_sms;
+    std::vector<LaunchPlan> plans;
+    for (int BN : {32, 64}) {
+        LaunchPlan shared;
+        for (const I8Job &jb : jobs) {
+            const int nclen = 2 * jb.nc10 + 1;
+            const long ncsize = (long)nclen * nclen;
+            if ((nclen <= 32 ? 32 : 64) != BN) continue;
+            if (jb.nanchors == 0) {
+                if ((rc = cuda_check(c, cudaMemsetAsync(jb.lag_out, 0, sizeof(double) * ncsize, c->stream), "zero lag")))
+                    return rc;
+                continue;
+            }
+            Planned p;
+            p.job = &jb;
+            p.bn = BN;
+            p.mt = (nclen + BM - 1) / BM;
+            p.nt = (nclen + BN - 1) / BN;
+            p.nch = choose_chunks(jb.k, (long)jb.nanchors * p.mt * p.nt, c->num_sms, ncsize, max_chunk);
+            p.chunk = ((jb.k + p.nch - 1) / p.nch + KB_B - 1) / KB_B * KB_B;
+            p.nch = (jb.k + p.chunk - 1) / p.chunk;
+            p.partial_bytes = (sizeof(double) * (size_t)jb.nanchors * p.nch * ncsize + 255) / 256 * 256;
+            const long ni = (long)jb.nanchors * p.mt * p.nt * p.nch;
+            if (ni >= big_items) {
+                LaunchPlan lp;
+                lp.persistent = false;
+                lp.jobs.push_back(p);
+                lp.nitems = ni;
+                lp.partial_bytes = p.partial_bytes;
+                plans.push_back(lp);
+                continue;
+            }
+            if (!shared.jobs.empty() && shared.partial_bytes + p.partial_bytes > pcap) {
+                plans.push_back(shared);
+                shared = LaunchPlan();
+            }
+            shared.jobs.push_back(p);
+            shared.nitems += ni;
+            shared.partial_bytes += p.partial_bytes;
+        }
+        if (!shared.jobs.empty()) plans.push_back(shared);
     }
-    if (rc) return rc;
-    if ((rc = lag_reduce(c, (const double *)c->partial.p, (long)nA * nch, ncsize, lag_out))) return rc;
+    if (plans.empty()) return AMBER_OK;
+    // staging: every launch's descriptors and items, uploaded once
+    size_t stage_bytes = 0, pmax = 0;
+    for (LaunchPlan &lp : plans) {
+        lp.desc_off = stage_bytes;
+        stage_bytes += sizeof(JobDesc) * lp.jobs.size();
+        lp.item_off = stage_bytes;
+        stage_bytes = (stage_bytes + sizeof(Item) * lp.nitems + 127) / 128 * 128;
+        pmax = std::max(pmax, lp.partial_bytes);
+    }
+    if ((rc = ensure(c, c->partial, pmax, "partial lag tiles"))) return rc;
+    if ((rc = ensure(c, c->jobdesc, stage_bytes, "job list"))) return rc;
+    if (c->stage_bytes < stage_bytes) {
+        if ((rc = cuda_check(c, cudaStreamSynchronize(c->stream), "job staging"))) return rc;
+        if (c->stage) cudaFreeHost(c->stage);
+        c->stage = nullptr;
+        c->stage_bytes = 0;
+        if ((rc = cuda_check(c, cudaHostAlloc(&c->stage, stage_bytes, cudaHostAllocDefault), "job staging"))) return rc;
+        c->stage_bytes = stage_bytes;
+    }
+    // the staging area may still feed the previous run's upload
+    if ((rc = cuda_check(c, cudaStreamSynchronize(c->stream), "job staging"))) return rc;
+    for (LaunchPlan &lp : plans)
+        if ((rc = fill_launch(c, lp, (char *)c->stage))) return rc;
+    if ((rc = cuda_check(c, cudaMemcpyAsync(c->jobdesc.p, c->stage, stage_bytes, cudaMemcpyHostToDevice, c->stream),
+                         "job list upload")))
+        return rc;
+    for (LaunchPlan &lp : plans) {
+        const JobDesc *d_jobs = (const JobDesc *)((char *)c->jobdesc.p + lp.desc_off);
+        const Item *d_items = (const Item *)((char *)c->jobdesc.p + lp.item_off);
+        phase_begin(c, 1);
+        const long grid = lp.persistent ? c->num_sms : lp.nitems;
+        rc = lp.jobs[0].bn == 32 ? launch<32>(c, d_jobs, d_items, lp.nitems, grid, d_err)
+                                 : launch<64>(c, d_jobs, d_items, lp.nitems, grid, d_err);
+        phase_end(c);
+        if (rc) return rc;
+        const JobDesc *h_desc = (const JobDesc *)((char *)c->stage + lp.desc_off);
+        for (size_t i = 0; i < lp.jobs.size(); ++i) {
+            const I8Job &jb = *lp.jobs[i].job;
+            const long ncsize = (long)(2 * jb.nc10 + 1) * (2 * jb.nc10 + 1);
+            if ((rc = lag_reduce(c, h_desc[i].partial, (long)jb.nanchors * lp.jobs[i].nch, ncsize, jb.lag_out)))
+                return rc;
+        }
+    }
     int herr = 0;
     if ((rc = cuda_check(c, cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream),
                          "error flag read")))
@@ -585,6 +741,21 @@ int contract_i8(amber_cuda_ctx *c, const DigitMaps &m1, const DigitMaps &m2, con
     if ((rc = cuda_check(c, cudaStreamSynchronize(c->stream), "contract_i8"))) return rc;
     if (herr) return fail(c, AMBER_ERR_TIMEOUT, "int8 tensor-core contraction: a pipeline wait gave up (site %d)", herr);
     return AMBER_OK;
+}
+
+int contract_i8(amber_cuda_ctx *c, const DigitMaps &m1, const DigitMaps &m2, const DigitMaps &m3, long k, long kp,
+                double *lag_out)
+{
+    std::vector<I8Job> jobs(1);
+    I8Job &jb = jobs[0];
+    jb.m1 = m1; jb.m2 = m2; jb.m3 = m3;
+    jb.k = k; jb.kp = kp;
+    jb.nc = (int)c->nc; jb.nc10 = c->nc10;
+    jb.anchors = (const int *)c->d_anchors.p;
+    jb.weight = (const int *)c->d_weight.p;
+    jb.nanchors = (int)c->anchors.size();
+    jb.lag_out = lag_out;
+    return contract_i8_jobs(c, jobs);
 }
 
 }  // namespace amber
