@@ -37,6 +37,7 @@ EXPORTS = (
     "amber_cuda_set_channels", "amber_cuda_calcr", "amber_cuda_ng1", "amber_cuda_triangle_v1",
     "amber_cuda_triangle_v2", "amber_cuda_triangles", "amber_cuda_triangles_run", "amber_cuda_triangles_fetch",
     "amber_cuda_last_run_stats", "amber_cuda_last_run_breakdown", "amber_cuda_grid_vis",
+    "amber_cuda_enqueue", "amber_cuda_wait", "amber_cuda_result", "amber_cuda_engine_stats",
 )
 
 
@@ -44,6 +45,24 @@ class AmberError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"libamber_cuda error {code} ({ERRORS.get(code, '?')}): {msg}")
         self.code = code
+
+
+class Request(ctypes.Structure):
+    _fields_ = [("N1", ctypes.c_long), ("nc", ctypes.c_long), ("Du", ctypes.c_double), ("flag_key", ctypes.c_int),
+                ("re_im", ctypes.POINTER(ctypes.c_double)), ("ntig", ctypes.POINTER(ctypes.c_double)),
+                ("Nr", ctypes.c_int), ("ULow", ctypes.POINTER(ctypes.c_double)),
+                ("UHigh", ctypes.POINTER(ctypes.c_double)), ("nc10", ctypes.c_int), ("uf_nc", ctypes.c_int),
+                ("uf_chans", ctypes.POINTER(ctypes.c_int)), ("want_v2", ctypes.c_int)]
+
+
+class EngineInfo(ctypes.Structure):
+    _fields_ = [("requests_done", ctypes.c_long), ("rounds", ctypes.c_long), ("contraction_launches", ctypes.c_long),
+                ("max_active", ctypes.c_long), ("queued", ctypes.c_long), ("active", ctypes.c_long),
+                ("peak_bytes", ctypes.c_size_t), ("budget_bytes", ctypes.c_size_t), ("products", ctypes.c_double),
+                ("busy_ms", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 class Opts(ctypes.Structure):
@@ -97,6 +116,10 @@ def load_library():
     L.amber_cuda_grid_vis.argtypes = [_vp, ctypes.c_long, ctypes.c_long, ctypes.c_double, ctypes.c_double,
                                       ctypes.c_float, ctypes.c_int, ctypes.c_long, ctypes.c_long, ctypes.c_long, _fp,
                                       _fp, _dp, _dp]
+    L.amber_cuda_enqueue.argtypes = [_vp, ctypes.POINTER(Request), _i64p]
+    L.amber_cuda_wait.argtypes = [_vp, ctypes.c_int64, ctypes.c_int, _ip]
+    L.amber_cuda_result.argtypes = [_vp, ctypes.c_int64, ctypes.c_int, _dp, _dp, _i64p, _dp, _dp]
+    L.amber_cuda_engine_stats.argtypes = [_vp, ctypes.POINTER(EngineInfo)]
     _lib = L
     return L
 
@@ -269,6 +292,61 @@ class Estimator:
                                                 int(flag_key), g, npar, nstokes, _ptr(randpar, _fp), _ptr(data, _fp),
                                                 _ptr(ri, _dp), _ptr(nt, _dp)))
         return ri[..., 0] + 1j * ri[..., 1], nt
+
+
+def _request_of(real, want_v2):
+    """Request struct for a synth.Realisation, with the numpy buffers it points to (keep them alive
+    until enqueue returns: the library copies them)."""
+    ri = np.ascontiguousarray(real.gv, dtype=np.complex128).view(np.float64)
+    nt = np.ascontiguousarray(real.counts, dtype=np.float64)
+    lo = np.ascontiguousarray(real.ulow, dtype=np.float64)
+    hi = np.ascontiguousarray(real.uhigh, dtype=np.float64)
+    uf = np.ascontiguousarray(real.uf_chans if real.flag_key == 1 else np.zeros(1), dtype=np.int32)
+    q = Request(real.gv.shape[0], real.gv.shape[2], float(real.du), int(real.flag_key), _ptr(ri, _dp), _ptr(nt, _dp),
+                len(lo), _ptr(lo, _dp), _ptr(hi, _dp), int(real.nc10), len(uf) if real.flag_key == 1 else 0,
+                _ptr(uf, _ip), int(bool(want_v2)))
+    return q, (ri, nt, lo, hi, uf)
+
+
+class Engine:
+    """Batched requests on one context: enqueue realisations (any mix of sizes), wait for them,
+    fetch their results.  The library's worker thread admits requests by HBM footprint and runs
+    the map-set batches of all admitted requests together (amber_cuda_enqueue)."""
+
+    def __init__(self, est: Estimator):
+        self.est = est
+        self._L = est._L
+
+    def enqueue(self, real, want_v2=True) -> int:
+        q, keep = _request_of(real, want_v2)
+        t = ctypes.c_int64()
+        self.est._check(self._L.amber_cuda_enqueue(self.est._h, ctypes.byref(q), ctypes.byref(t)))
+        del keep
+        return t.value
+
+    def wait(self, ticket: int, timeout_ms: int = -1) -> int:
+        n = ctypes.c_int()
+        self.est._check(self._L.amber_cuda_wait(self.est._h, ticket, timeout_ms, ctypes.byref(n)))
+        return n.value
+
+    def result(self, ticket: int, real, want_v2=True):
+        """(rdata, bldnu, numdnu, numtri, latency_ms) of a finished request; FP64 lag arrays
+        [ntri, nclen²], int64 counts."""
+        n = self.wait(ticket)
+        nclen = 2 * real.nc10 + 1
+        rd = np.zeros((max(n, 1), 4))
+        bl = np.zeros((max(n, 1), nclen * nclen))
+        nd = np.zeros((max(n, 1), nclen * nclen), dtype=np.int64)
+        nt = np.zeros((max(n, 1), nclen * nclen)) if want_v2 else None
+        lat = ctypes.c_double()
+        self.est._check(self._L.amber_cuda_result(self.est._h, ticket, max(n, 1), _ptr(rd, _dp), _ptr(bl, _dp),
+                                                  _ptr(nd, _i64p), _ptr(nt, _dp), ctypes.byref(lat)))
+        return rd[:n], bl[:n], nd[:n], (None if nt is None else nt[:n]), lat.value
+
+    def stats(self) -> dict:
+        i = EngineInfo()
+        self.est._check(self._L.amber_cuda_engine_stats(self.est._h, ctypes.byref(i)))
+        return i.as_dict()
 
 
 def estimate(real, precision="mixed", version=1, tri_subset=None, est: Estimator | None = None):

@@ -190,15 +190,223 @@ int upload_grid(amber_cuda_ctx *c, long N1, long nc, double Du, int flag_key, co
     return cuda_check(c, cudaStreamSynchronize(c->stream), "grid upload");
 }
 
-// Which rings each r1 group needs, for a list of triangles.
-struct Group {
-    int r1;
-    long ng;
-    std::vector<int> tris;  // indices into the caller's list
-};
-
 }  // namespace
+
+long ring_ng1(double uhigh, double du) { return ng1_of(uhigh, du); }
+
+std::vector<int> closed_triangles(const std::vector<double> &ulow, const std::vector<double> &uhigh)
+{
+    const int Nr = (int)ulow.size();
+    std::vector<double> ua(Nr);
+    for (int i = 0; i < Nr; ++i)  // amber_funcs.c:2065, as amber_cuda_set_rings
+        ua[i] = (2. / 3.) * (pow(uhigh[i], 3.) - pow(ulow[i], 3.)) / (pow(uhigh[i], 2.) - pow(ulow[i], 2.));
+    std::vector<int> tri;
+    for (int r1 = 0; r1 < Nr; ++r1)
+        for (int r2 = 0; r2 <= r1; ++r2)
+            for (int r3 = 0; r3 <= r2; ++r3)
+                if (closed(ua, r1, r2, r3)) {
+                    tri.push_back(r1);
+                    tri.push_back(r2);
+                    tri.push_back(r3);
+                }
+    return tri;
+}
+
+// ---- one realisation's triangles, run in map-set batches ----
+
+int run_begin(amber_cuda_ctx *c, RunState &st, int ntri, const int *tri, int want_v2)
+{
+    if (!c || ntri < 0 || (ntri > 0 && !tri)) return AMBER_ERR_ARG;
+    int rc = check_ready(c, true);
+    if (rc) return rc;
+    for (int t = 0; t < ntri; ++t) {
+        int r1 = tri[3 * t], r2 = tri[3 * t + 1], r3 = tri[3 * t + 2];
+        if (r1 < 0 || r1 >= c->Nr || r2 < 0 || r2 >= c->Nr || r3 < 0 || r3 >= c->Nr)
+            return fail(c, AMBER_ERR_ARG, "triangle %d has a ring outside [0, %d)", t, c->Nr);
+    }
+    cudaSetDevice(c->device);
+    const int nclen = 2 * c->nc10 + 1;
+    const long ncsize = (long)nclen * nclen;
+    if ((rc = ensure(c, c->results, sizeof(double) * 2 * ncsize * std::max(1, ntri), "results"))) return rc;
+    st = RunState();
+    st.tri.assign(tri, tri + 3 * ntri);
+    st.want_v2 = want_v2;
+    // group by r1: every ring of a group lives on the group's Ng1 grid
+    for (int t = 0; t < ntri; ++t) {
+        int r1 = tri[3 * t];
+        long ng = ng1_of(c->uhigh[r1], c->Du);
+        auto it = std::find_if(st.groups.begin(), st.groups.end(), [&](const RunState::Group &g) { return g.r1 == r1; });
+        if (it == st.groups.end()) {
+            st.groups.push_back(RunState::Group{r1, ng, {}});
+            it = st.groups.end() - 1;
+        }
+        it->tris.push_back(t);
+    }
+    return AMBER_OK;
+}
+
+size_t map_slot_bytes(int precision, long ng, long nc, int want_v2)
+{
+    const size_t vbytes = precision == AMBER_PREC_FP64 ? 8 : (precision == AMBER_PREC_MIXED ? 7 : 4);
+    const long kalign = precision == AMBER_PREC_MIXED ? 128 : 64;
+    const long k = ng * ng, kp = (k + kalign - 1) / kalign * kalign;
+    const size_t per_pass = vbytes * (size_t)nc * kp + 8 * (size_t)nc;
+    // + the map builder's column-pass intermediate (double2 per ring row, column and channel)
+    const size_t y = sizeof(double2) * (size_t)ng * (size_t)(ng / 3 + 1) * (size_t)nc;
+    return per_pass * (want_v2 ? 2 : 1) + y;
+}
+
+int run_next_batch(amber_cuda_ctx *c, RunState &st, std::vector<I8Job> *jobs)
+{
+    int rc;
+    while (st.gi < st.groups.size() && st.ti >= st.groups[st.gi].tris.size()) {
+        ++st.gi;
+        st.ti = 0;
+    }
+    if (st.gi >= st.groups.size()) return 0;
+    const RunState::Group &g = st.groups[st.gi];
+    const int *tri = st.tri.data();
+    const int want_v2 = st.want_v2;
+    const int prec = c->precision;
+    const int nclen = 2 * c->nc10 + 1;
+    const long ncsize = (long)nclen * nclen;
+    double *res = (double *)c->results.p;
+    const size_t vbytes = prec == AMBER_PREC_FP64 ? 8 : (prec == AMBER_PREC_MIXED ? 7 : 4);
+    const long kalign = prec == AMBER_PREC_MIXED ? 128 : 64;
+    const long k = g.ng * g.ng, kp = (k + kalign - 1) / kalign * kalign;
+    const size_t per_slot = vbytes * (size_t)c->nc * kp + 8 * (size_t)c->nc;
+    // The next batch of the group: triangles whose ring union fits the budget.
+    size_t spare = c->budget > c->held ? c->budget - c->held : 0;
+    spare += c->maps_d.bytes + c->maps_i.bytes + c->y.bytes;
+    const size_t reserve = (size_t)64 << 20;
+    const long cap_slots = (long)((spare > reserve ? spare - reserve : 0) /
+                                  (map_slot_bytes(prec, g.ng, c->nc, want_v2) + 1));
+    if (cap_slots < 3) return fail(c, AMBER_ERR_OOM, "maps of one triangle (Ng1=%ld) exceed the budget", g.ng);
+    std::vector<int> batch;
+    std::set<int> rings;
+    while (st.ti < g.tris.size()) {
+        int t = g.tris[st.ti];
+        std::set<int> u = rings;
+        u.insert(tri[3 * t]);
+        u.insert(tri[3 * t + 1]);
+        u.insert(tri[3 * t + 2]);
+        if ((long)u.size() > cap_slots) break;
+        rings = u;
+        batch.push_back(t);
+        ++st.ti;
+    }
+    MapSet ms;
+    ms.ng = g.ng;
+    ms.k = k;
+    ms.kp = kp;
+    for (int i = 0; i < 256; ++i) ms.slot_of_ring[i] = -1;
+    for (int r : rings) {
+        ms.slot_of_ring[r] = (int)ms.ring_of_slot.size();
+        ms.ring_of_slot.push_back(r);
+    }
+    ms.nslots = (int)ms.ring_of_slot.size();
+    const size_t nvals = (size_t)ms.nslots * c->nc * kp, nrows = (size_t)ms.nslots * c->nc;
+    if ((rc = ensure(c, c->maps_d, per_slot * ms.nslots, "ring maps"))) return rc;
+    if (want_v2 && (rc = ensure(c, c->maps_i, per_slot * ms.nslots, "ring mask maps"))) return rc;
+    // carve one map set (D or I) out of its buffer
+    auto carve = [&](void *base, MapJob &job, DigitMaps *dm_base) {
+        char *p = (char *)base;
+        if (prec == AMBER_PREC_FP64) {
+            job.out_f64 = (double *)p;
+        } else if (prec == AMBER_PREC_BF16X3) {
+            job.out_hi = (uint16_t *)p;
+            job.out_lo = (uint16_t *)p + nvals;
+        } else {
+            job.out_f32 = (float *)p;
+            job.d0 = (int8_t *)(p + 4 * nvals);
+            job.d1 = job.d0 + nvals;
+            job.d2 = job.d1 + nvals;
+            job.expo = (int *)(p + 7 * nvals);
+            job.rowmax = (unsigned *)(job.expo + nrows);
+            if (dm_base) {
+                dm_base->f32 = job.out_f32;
+                dm_base->d0 = job.d0;
+                dm_base->d1 = job.d1;
+                dm_base->d2 = job.d2;
+                dm_base->expo = job.expo;
+            }
+        }
+    };
+    std::vector<I8Job> local;
+    std::vector<I8Job> *jl = jobs ? jobs : &local;
+    DigitMaps dmaps[2];
+    for (int pass = 0; pass < (want_v2 ? 2 : 1); ++pass) {
+        MapJob job{};
+        job.src = pass == 0 ? c->grid.p : c->mask.p;
+        job.src_complex = pass == 0;
+        job.n1 = c->N1;
+        job.nc = c->nc;
+        job.chan_base = 0;
+        job.nch = c->nc;
+        job.ng = g.ng;
+        job.kp = kp;
+        job.nslots = ms.nslots;
+        for (int r : ms.ring_of_slot) {
+            job.lo.push_back(c->ulow[r]);
+            job.hi.push_back(c->uhigh[r]);
+        }
+        carve(pass == 0 ? c->maps_d.p : c->maps_i.p, job, &dmaps[pass]);
+        if (job.rowmax &&
+            (rc = cuda_check(c, cudaMemsetAsync(job.rowmax, 0, sizeof(unsigned) * nrows, c->stream),
+                             "row max reset")))
+            return rc;
+        phase_begin(c, 0);
+        rc = build_maps(c, job);
+        phase_end(c);
+        if (rc) return rc;
+    }
+    for (int t : batch) {
+        const size_t s1 = ms.slot_of_ring[tri[3 * t]], s2 = ms.slot_of_ring[tri[3 * t + 1]],
+                     s3 = ms.slot_of_ring[tri[3 * t + 2]];
+        const size_t ss = (size_t)c->nc * kp;
+        for (int pass = 0; pass < (want_v2 ? 2 : 1); ++pass) {
+            void *base = pass == 0 ? c->maps_d.p : c->maps_i.p;
+            double *lag = res + ((size_t)t * 2 + pass) * ncsize;
+            if (prec == AMBER_PREC_MIXED) {
+                const DigitMaps &b = dmaps[pass];
+                auto slot = [&](size_t s) {
+                    DigitMaps d;
+                    d.f32 = b.f32 + s * ss;
+                    d.d0 = b.d0 + s * ss;
+                    d.d1 = b.d1 + s * ss;
+                    d.d2 = b.d2 + s * ss;
+                    d.expo = b.expo + s * c->nc;
+                    return d;
+                };
+                I8Job jb;
+                jb.m1 = slot(s1); jb.m2 = slot(s2); jb.m3 = slot(s3);
+                jb.k = k; jb.kp = kp;
+                jb.nc = (int)c->nc; jb.nc10 = c->nc10;
+                jb.anchors = (const int *)c->d_anchors.p;
+                jb.weight = (const int *)c->d_weight.p;
+                jb.nanchors = (int)c->anchors.size();
+                jb.lag_out = lag;
+                jl->push_back(jb);
+                rc = AMBER_OK;
+            } else if (prec == AMBER_PREC_BF16X3) {
+                const uint16_t *hi = (const uint16_t *)base;
+                const uint16_t *lo = hi + nvals;
+                rc = contract_bf16x3(c, hi + s1 * ss, lo + s1 * ss, hi + s2 * ss, lo + s2 * ss, hi + s3 * ss,
+                                     lo + s3 * ss, k, kp, lag);
+            } else {
+                const double *m = (const double *)base;
+                rc = contract_fp64(c, m + s1 * ss, m + s2 * ss, m + s3 * ss, k, kp, lag);
+            }
+            if (rc) return rc;
+        }
+        c->last_products += (double)c->total_vcp * (double)k * (want_v2 ? 2.0 : 1.0);
+    }
+    if (!local.empty() && (rc = contract_i8_jobs(c, local))) return rc;
+    return 1;
+}
+
 }  // namespace amber
+
 
 using namespace amber;
 
@@ -253,6 +461,7 @@ int amber_cuda_create(const amber_cuda_opts *opts, amber_cuda_ctx **out)
 void amber_cuda_destroy(amber_cuda_ctx *c)
 {
     if (!c) return;
+    amber::engine_shutdown(c);
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);
     DevBuf *bufs[] = {&c->grid, &c->mask, &c->d_weight, &c->d_anchors, &c->y, &c->maps_d, &c->maps_i,
@@ -445,173 +654,22 @@ int amber_cuda_calcr(amber_cuda_ctx *c, int max_tri, int *rcount, double *rdata)
 
 int amber_cuda_triangles_run(amber_cuda_ctx *c, int ntri, const int *tri, int want_v2)
 {
-    if (!c || ntri < 0 || (ntri > 0 && !tri)) return AMBER_ERR_ARG;
-    int rc = check_ready(c, true);
+    amber::RunState st;
+    int rc = amber::run_begin(c, st, ntri, tri, want_v2);
     if (rc) return rc;
-    for (int t = 0; t < ntri; ++t) {
-        int r1 = tri[3 * t], r2 = tri[3 * t + 1], r3 = tri[3 * t + 2];
-        if (r1 < 0 || r1 >= c->Nr || r2 < 0 || r2 >= c->Nr || r3 < 0 || r3 >= c->Nr)
-            return fail(c, AMBER_ERR_ARG, "triangle %d has a ring outside [0, %d)", t, c->Nr);
-    }
-    cudaSetDevice(c->device);
-    const int nclen = 2 * c->nc10 + 1;
-    const long ncsize = (long)nclen * nclen;
-    if ((rc = ensure(c, c->results, sizeof(double) * 2 * ncsize * std::max(1, ntri), "results"))) return rc;
-    double *res = (double *)c->results.p;
-
-    // group by r1: every ring of a group lives on the group's Ng1 grid
-    std::vector<Group> groups;
-    for (int t = 0; t < ntri; ++t) {
-        int r1 = tri[3 * t];
-        long ng = ng1_of(c->uhigh[r1], c->Du);
-        auto it = std::find_if(groups.begin(), groups.end(), [&](const Group &g) { return g.r1 == r1; });
-        if (it == groups.end()) {
-            groups.push_back(Group{r1, ng, {}});
-            it = groups.end() - 1;
-        }
-        it->tris.push_back(t);
-    }
-    const int prec = c->precision;
-    // bytes per map value: FP64; int8 path: FP32 plane + 3 digit planes; bf16 path: hi + lo
-    const size_t vbytes = prec == AMBER_PREC_FP64 ? 8 : (prec == AMBER_PREC_MIXED ? 7 : 4);
-    const long kalign = prec == AMBER_PREC_MIXED ? 128 : 64;
     c->last_products = 0;
     c->phase_used = 0;
     c->launches = 0;
     c->contractions = 0;
     cudaEventRecord(c->ev0, c->stream);
-    for (const Group &g : groups) {
-        const long k = g.ng * g.ng, kp = (k + kalign - 1) / kalign * kalign;
-        const size_t per_slot = vbytes * (size_t)c->nc * kp + 8 * (size_t)c->nc;
-        // Process the group's triangles in batches whose ring union fits the budget.
-        size_t spare = c->budget > c->held ? c->budget - c->held : 0;
-        spare += c->maps_d.bytes + c->maps_i.bytes;
-        size_t reserve = (size_t)64 << 20;
-        long cap_slots = (long)((spare > reserve ? spare - reserve : 0) / (per_slot * (want_v2 ? 2 : 1) + 1));
-        if (cap_slots < 3) return fail(c, AMBER_ERR_OOM, "maps of one triangle (Ng1=%ld) exceed the budget", g.ng);
-        size_t ti = 0;
-        while (ti < g.tris.size()) {
-            std::vector<int> batch;
-            std::set<int> rings;
-            while (ti < g.tris.size()) {
-                int t = g.tris[ti];
-                std::set<int> u = rings;
-                u.insert(tri[3 * t]);
-                u.insert(tri[3 * t + 1]);
-                u.insert(tri[3 * t + 2]);
-                if ((long)u.size() > cap_slots) break;
-                rings = u;
-                batch.push_back(t);
-                ++ti;
-            }
-            MapSet ms;
-            ms.ng = g.ng;
-            ms.k = k;
-            ms.kp = kp;
-            for (int i = 0; i < 256; ++i) ms.slot_of_ring[i] = -1;
-            for (int r : rings) {
-                ms.slot_of_ring[r] = (int)ms.ring_of_slot.size();
-                ms.ring_of_slot.push_back(r);
-            }
-            ms.nslots = (int)ms.ring_of_slot.size();
-            const size_t nvals = (size_t)ms.nslots * c->nc * kp, nrows = (size_t)ms.nslots * c->nc;
-            if ((rc = ensure(c, c->maps_d, per_slot * ms.nslots, "ring maps"))) return rc;
-            if (want_v2 && (rc = ensure(c, c->maps_i, per_slot * ms.nslots, "ring mask maps"))) return rc;
-            // carve one map set (D or I) out of its buffer
-            auto carve = [&](void *base, MapJob &job, DigitMaps *dm_base) {
-                char *p = (char *)base;
-                if (prec == AMBER_PREC_FP64) {
-                    job.out_f64 = (double *)p;
-                } else if (prec == AMBER_PREC_BF16X3) {
-                    job.out_hi = (uint16_t *)p;
-                    job.out_lo = (uint16_t *)p + nvals;
-                } else {
-                    job.out_f32 = (float *)p;
-                    job.d0 = (int8_t *)(p + 4 * nvals);
-                    job.d1 = job.d0 + nvals;
-                    job.d2 = job.d1 + nvals;
-                    job.expo = (int *)(p + 7 * nvals);
-                    job.rowmax = (unsigned *)(job.expo + nrows);
-                    if (dm_base) {
-                        dm_base->f32 = job.out_f32;
-                        dm_base->d0 = job.d0;
-                        dm_base->d1 = job.d1;
-                        dm_base->d2 = job.d2;
-                        dm_base->expo = job.expo;
-                    }
-                }
-            };
-            DigitMaps dmaps[2];
-            for (int pass = 0; pass < (want_v2 ? 2 : 1); ++pass) {
-                MapJob job{};
-                job.src = pass == 0 ? c->grid.p : c->mask.p;
-                job.src_complex = pass == 0;
-                job.n1 = c->N1;
-                job.nc = c->nc;
-                job.chan_base = 0;
-                job.nch = c->nc;
-                job.ng = g.ng;
-                job.kp = kp;
-                job.nslots = ms.nslots;
-                for (int r : ms.ring_of_slot) {
-                    job.lo.push_back(c->ulow[r]);
-                    job.hi.push_back(c->uhigh[r]);
-                }
-                carve(pass == 0 ? c->maps_d.p : c->maps_i.p, job, &dmaps[pass]);
-                if (job.rowmax &&
-                    (rc = cuda_check(c, cudaMemsetAsync(job.rowmax, 0, sizeof(unsigned) * nrows, c->stream),
-                                     "row max reset")))
-                    return rc;
-                phase_begin(c, 0);
-                rc = build_maps(c, job);
-                phase_end(c);
-                if (rc) return rc;
-            }
-            std::vector<I8Job> jobs;  // mixed path: the whole batch goes to the persistent kernel at once
-            for (int t : batch) {
-                const size_t s1 = ms.slot_of_ring[tri[3 * t]], s2 = ms.slot_of_ring[tri[3 * t + 1]],
-                             s3 = ms.slot_of_ring[tri[3 * t + 2]];
-                const size_t ss = (size_t)c->nc * kp;
-                for (int pass = 0; pass < (want_v2 ? 2 : 1); ++pass) {
-                    void *base = pass == 0 ? c->maps_d.p : c->maps_i.p;
-                    double *lag = res + ((size_t)t * 2 + pass) * ncsize;
-                    if (prec == AMBER_PREC_MIXED) {
-                        const DigitMaps &b = dmaps[pass];
-                        auto slot = [&](size_t s) {
-                            DigitMaps d;
-                            d.f32 = b.f32 + s * ss;
-                            d.d0 = b.d0 + s * ss;
-                            d.d1 = b.d1 + s * ss;
-                            d.d2 = b.d2 + s * ss;
-                            d.expo = b.expo + s * c->nc;
-                            return d;
-                        };
-                        I8Job jb;
-                        jb.m1 = slot(s1); jb.m2 = slot(s2); jb.m3 = slot(s3);
-                        jb.k = k; jb.kp = kp;
-                        jb.nc = (int)c->nc; jb.nc10 = c->nc10;
-                        jb.anchors = (const int *)c->d_anchors.p;
-                        jb.weight = (const int *)c->d_weight.p;
-                        jb.nanchors = (int)c->anchors.size();
-                        jb.lag_out = lag;
-                        jobs.push_back(jb);
-                        rc = AMBER_OK;
-                    } else if (prec == AMBER_PREC_BF16X3) {
-                        const uint16_t *hi = (const uint16_t *)base;
-                        const uint16_t *lo = hi + nvals;
-                        rc = contract_bf16x3(c, hi + s1 * ss, lo + s1 * ss, hi + s2 * ss, lo + s2 * ss, hi + s3 * ss,
-                                             lo + s3 * ss, k, kp, lag);
-                    } else {
-                        const double *m = (const double *)base;
-                        rc = contract_fp64(c, m + s1 * ss, m + s2 * ss, m + s3 * ss, k, kp, lag);
-                    }
-                    if (rc) return rc;
-                }
-                c->last_products += (double)c->total_vcp * (double)k * (want_v2 ? 2.0 : 1.0);
-            }
-            if (!jobs.empty() && (rc = contract_i8_jobs(c, jobs))) return rc;
-        }
+    const bool mixed = c->precision == AMBER_PREC_MIXED;
+    std::vector<amber::I8Job> jobs;
+    while ((rc = amber::run_next_batch(c, st, mixed ? &jobs : nullptr)) == 1) {
+        // mixed path: the whole batch (every triangle and pass) in persistent launches
+        if (mixed && (rc = amber::contract_i8_jobs(c, jobs))) return rc;
+        jobs.clear();
     }
+    if (rc < 0) return rc;
     cudaEventRecord(c->ev1, c->stream);
     if ((rc = cuda_check(c, cudaEventSynchronize(c->ev1), "triangle run"))) return rc;
     if ((rc = cuda_check(c, cudaGetLastError(), "triangle run"))) return rc;

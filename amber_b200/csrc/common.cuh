@@ -30,6 +30,8 @@ struct MapSet {
     int slot_of_ring[256];
 };
 
+struct Engine;  // request engine (engine.cu)
+
 }  // namespace amber
 
 struct amber_cuda_ctx {
@@ -79,6 +81,7 @@ struct amber_cuda_ctx {
     amber::DevBuf jobdesc; // contraction job descriptors and work items
     void *stage = nullptr; // pinned host staging of the job descriptors
     size_t stage_bytes = 0;
+    amber::Engine *engine = nullptr;  // batched requests, created on the first enqueue
 
     // per-phase device timing of the last run (CUDA events on the launch stream)
     struct PhaseEv {
@@ -161,6 +164,34 @@ struct I8Job {
 // All jobs in as few persistent launches as the partial-tile memory allows (jobs of
 // different realisations may share a launch); each job's result depends on the job only.
 int contract_i8_jobs(amber_cuda_ctx *c, const std::vector<I8Job> &jobs);
+
+// One realisation's list of triangles, run in map-set batches: the triangles are grouped
+// by r1 (one Ng1 grid per group) and each group is cut into batches whose ring maps fit
+// the context's budget.
+struct RunState {
+    struct Group {
+        int r1;
+        long ng;
+        std::vector<int> tris;  // indices into tri
+    };
+    std::vector<int> tri;  // 3 rings per triangle
+    int want_v2 = 0;
+    std::vector<Group> groups;
+    size_t gi = 0, ti = 0;  // next group, next triangle in it
+};
+int run_begin(amber_cuda_ctx *c, RunState &st, int ntri, const int *tri, int want_v2);
+// Builds the ring maps of the next batch.  Mixed precision: appends the batch's jobs to
+// *jobs for the caller to contract (or contracts them at once when jobs is null); other
+// precisions contract here.  Returns 1 after a batch, 0 when the run is complete, <0 on error.
+int run_next_batch(amber_cuda_ctx *c, RunState &st, std::vector<I8Job> *jobs);
+// Device bytes of one ring slot of a map batch on an ng grid (D and, for v2, mask maps,
+// plus the map builder's intermediate).
+size_t map_slot_bytes(int precision, long ng, long nc, int want_v2);
+// Ng1 of a ring (amber.c:193-197) and calCR's closed triangles (r1 ≥ r2 ≥ r3, in its order).
+long ring_ng1(double uhigh, double du);
+std::vector<int> closed_triangles(const std::vector<double> &ulow, const std::vector<double> &uhigh);
+// Stops the context's request engine (pending requests finish, queued ones are dropped).
+void engine_shutdown(amber_cuda_ctx *c);
 // lag[d] = Σ_u partial[u][d] (compensated, fixed order).
 int lag_reduce(amber_cuda_ctx *c, const double *partial, long nunits, long ncsize, double *lag);
 // Σ_x a·b·c over n points (FP64, deterministic) into out[0].

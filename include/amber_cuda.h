@@ -144,6 +144,61 @@ AMBER_API int amber_cuda_grid_vis(amber_cuda_ctx *ctx, long NN, long nc, double 
                         long ngroups, long npar, long nstokes, const float *randpar, const float *data,
                         double *re_im_out, double *ntig_out);
 
+/* ---- batched requests: ensembles of realisations and estimation streams.
+ * The reference estimates one realisation per process run (amber.c:21-335);
+ * these calls are the batch form of amber_cuda_load_grid_packed +
+ * amber_cuda_set_rings + amber_cuda_set_channels + amber_cuda_calcr +
+ * amber_cuda_triangles for many realisations of uneven size at once.
+ *
+ * amber_cuda_enqueue copies the request's inputs (the caller may free them on
+ * return) and queues it; a worker thread of the context runs it.  Requests are
+ * admitted first come first served while their estimated device footprint
+ * fits the context's HBM budget; the map-set batches of all admitted requests
+ * run together in shared contraction launches, round by round, and a request
+ * that arrives meanwhile joins at the next round.  A request's results do not
+ * depend on what it shares the GPU with.  All triangles calCR closes are
+ * estimated (v2 adds the sampling-mask sums).  While requests are pending,
+ * make no other call on the context than these four.
+ *
+ * amber_cuda_wait blocks until the request is done (timeout_ms < 0: no limit;
+ * AMBER_ERR_TIMEOUT when the limit passes first, the request keeps running)
+ * and gives its triangle count; a failed request returns its error.
+ * amber_cuda_result then copies the outputs into caller buffers and forgets
+ * the request: rdata [ntri][4] as amber_cuda_calcr, bldnu and numtri (v2)
+ * [ntri][nclen²] FP64, numdnu [ntri][nclen²] int64, and the request's
+ * latency in ms from enqueue to completion.  Any output pointer may be NULL. */
+typedef struct amber_cuda_request {
+    long N1, nc;
+    double Du;
+    int flag_key;
+    const double *re_im; /* [N1·(N1/2+1)][nc] complex as (re, im), as amber_cuda_load_grid_packed */
+    const double *ntig;  /* [N1·(N1/2+1)][nc] sampling counts */
+    int Nr;
+    const double *ULow, *UHigh;
+    int nc10;
+    int uf_nc;            /* unflagged channel list when flag_key == 1 */
+    const int *uf_chans;
+    int want_v2;
+} amber_cuda_request;
+
+typedef struct amber_cuda_engine_info {
+    long requests_done;
+    long rounds;               /* scheduling rounds run */
+    long contraction_launches; /* contraction-kernel launches over all rounds */
+    long max_active;           /* most requests admitted at once */
+    long queued, active;       /* now */
+    size_t peak_bytes;         /* most footprint admitted at once */
+    size_t budget_bytes;       /* the engine's share of the context budget */
+    double products;           /* lag-triple products of the finished requests */
+    double busy_ms;            /* wall time spent in rounds */
+} amber_cuda_engine_info;
+
+AMBER_API int amber_cuda_enqueue(amber_cuda_ctx *ctx, const amber_cuda_request *req, int64_t *ticket);
+AMBER_API int amber_cuda_wait(amber_cuda_ctx *ctx, int64_t ticket, int timeout_ms, int *ntri);
+AMBER_API int amber_cuda_result(amber_cuda_ctx *ctx, int64_t ticket, int max_tri, double *rdata, double *bldnu,
+                                int64_t *numdnu, double *numtri, double *latency_ms);
+AMBER_API int amber_cuda_engine_stats(amber_cuda_ctx *ctx, amber_cuda_engine_info *info);
+
 /* ---- allocation-free FP64 lag contraction of one triangle.  No counterpart
  * in the reference: it exists for callers that own every device allocation
  * themselves — a process that reserves its HBM budget at start-up, or an
