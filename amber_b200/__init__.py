@@ -59,7 +59,8 @@ class EngineInfo(ctypes.Structure):
     _fields_ = [("requests_done", ctypes.c_long), ("rounds", ctypes.c_long), ("contraction_launches", ctypes.c_long),
                 ("max_active", ctypes.c_long), ("queued", ctypes.c_long), ("active", ctypes.c_long),
                 ("peak_bytes", ctypes.c_size_t), ("budget_bytes", ctypes.c_size_t), ("products", ctypes.c_double),
-                ("busy_ms", ctypes.c_double)]
+                ("busy_ms", ctypes.c_double), ("setup_ms", ctypes.c_double), ("maps_ms", ctypes.c_double),
+                ("contract_ms", ctypes.c_double), ("finish_ms", ctypes.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -268,14 +268,18 @@ void Engine::loop()
         std::vector<Request *> in_round;
         for (Request *r : round) {
             int rc = AMBER_OK;
+            double ta = now_ms();
             if (!r->started) rc = setup(r);
+            info.setup_ms += now_ms() - ta;
             if (!rc && run_finished(r->run)) {
                 finish(r);  // no triangles at all
                 continue;
             }
             if (!rc) {
+                ta = now_ms();
                 rc = run_next_batch(r->sub, r->run, &jobs);
                 rc = rc < 0 ? rc : AMBER_OK;
+                info.maps_ms += now_ms() - ta;
             }
             if (rc) {
                 fail_req(r, rc, r->sub ? r->sub->err : std::string("context creation failed"));
@@ -284,11 +288,14 @@ void Engine::loop()
             in_round.push_back(r);
         }
         int rc = AMBER_OK;
+        double tc = now_ms();
         if (!jobs.empty()) {
             const long before = owner->contractions;
             rc = contract_i8_jobs(owner, jobs);
             info.contraction_launches += owner->contractions - before;
         }
+        info.contract_ms += now_ms() - tc;
+        tc = now_ms();
         if (rc) {
             const std::string msg = owner->err;
             for (Request *r : in_round) fail_req(r, rc, msg);
@@ -296,6 +303,7 @@ void Engine::loop()
             for (Request *r : in_round)
                 if (run_finished(r->run)) finish(r);
         }
+        info.finish_ms += now_ms() - tc;
         info.rounds += 1;
         info.busy_ms += now_ms() - t0;
     }

@@ -21,7 +21,11 @@ per triangle total_vcp·Ng1², counted for the D and the I (mask) sums.
 * roofline — the contraction kernel, algorithmic flops (2 per product) per
   launch over its CUDA-event time, against the measured bf16 dense peak;
 * cpu_baseline — the reference's own OpenMP loop (oracle/_ref/ref_amber_fast,
-  its sources built unchanged) on the host cores over a bounded sample.
+  its sources built unchanged) on the host cores over a bounded sample;
+* ensemble — 64 realisations of uneven size through the request engine
+  (amber_cuda_enqueue), end to end, with mixed vs plain FP64 on a subset;
+* serving — a prefix of the Poisson request stream enqueued at its arrival
+  times: p50/p99 latency and throughput, FP64 one-at-a-time beside it.
 
 `--impl reference` times that same reference build as the reference arm.
 Multi-GPU: one process per GPU (torchrun), each rank runs its own realisation
@@ -163,6 +167,92 @@ def run_reference_arm(args):
     return 0
 
 
+def _engine_run(amber_b200, reals, precision, dev):
+    """All realisations through one context's request engine; returns (wall s, products, results, stats)."""
+    with amber_b200.Estimator(device=dev, precision=precision) as est:
+        eng = amber_b200.Engine(est)
+        p0 = eng.stats()["products"]
+        t0 = time.perf_counter()
+        tickets = [eng.enqueue(r, want_v2=True) for r in reals]
+        res = [eng.result(t, r, want_v2=True) for t, r in zip(tickets, reals)]
+        wall = time.perf_counter() - t0
+        st = eng.stats()
+    return wall, st["products"] - p0, res, st
+
+
+def ensemble_section(amber_b200, synth, dev):
+    """Batched ensemble: the 64 realisations of uneven size (sides 96-320, 24-160 channels, 10 %
+    flags, 12 bins) through the request engine, end to end (inputs from host memory, every lag
+    array back); plus mixed vs plain FP64 on a fixed subset of the same ensemble."""
+    specs = synth.config3_specs()
+    t_gen = time.perf_counter()
+    reals = [synth.from_spec(s) for s in specs]
+    t_gen = time.perf_counter() - t_gen
+    _engine_run(amber_b200, reals[48:49], "mixed", dev)  # warm-up (allocations, twiddles)
+    wall, prod, _, st = _engine_run(amber_b200, reals, "mixed", dev)
+    sub = [0, 16, 48]
+    sreals = [reals[i] for i in sub]
+    w_m, p_m, r_m, _ = _engine_run(amber_b200, sreals, "mixed", dev)
+    w_f, p_f, r_f, _ = _engine_run(amber_b200, sreals, "fp64", dev)
+    _, _, r_a, _ = _engine_run(amber_b200, sreals, "fp64_abs", dev)
+    err = 0.0
+    for m, f, a in zip(r_m, r_f, r_a):
+        err = max(err, float((np.abs(m[1] - f[1]) / (a[1] + 1e-300)).max()),
+                  float((np.abs(m[3] - f[3]) / (a[3] + 1e-300)).max()))
+        assert np.array_equal(m[2], f[2])  # counts exact
+    return {"workload": "ensemble: 64 realisations, sides {96,128,192,256,320}, 24-160 channels, 10 % flags, "
+                        "12 log bins 2..0.47*side, nc10=nc/2-1, v2, all closed triangles, seeds 100-163",
+            "value": prod / wall, "unit": UNIT, "products": prod, "wall_s": wall,
+            "timing": "end to end through amber_cuda_enqueue/wait/result from host memory (wall clock)",
+            "engine": {k: st[k] for k in ("rounds", "contraction_launches", "max_active", "peak_bytes", "busy_ms",
+                                          "setup_ms", "maps_ms", "contract_ms", "finish_ms")},
+            "fp64_plain": {"sample": "realisations 0, 16, 48 of the ensemble (sides 256/192/96), same engine",
+                           "value": p_f / w_f, "mixed_same_sample": p_m / w_m, "speedup": (p_m / w_m) / (p_f / w_f),
+                           "max_rel_err_vs_fp64": err, "err_scale": "sum of |products| per lag cell"},
+            "generation_s": t_gen}
+
+
+def serving_section(amber_b200, synth, dev, n=8):
+    """Serving stream: the first n requests of the Poisson stream (50 req/s; sides {64..384},
+    16-256 channels, 6-20 bins) enqueued at their arrival times; latency = arrival to result
+    ready.  The stream as specified is far beyond one GPU's capacity (~1.5e17 products arriving
+    in 39 s), so only a prefix runs; the plain FP64 one-at-a-time path is timed on two small
+    requests of the prefix."""
+    reqs = synth.config5_requests()[:n]
+    reals = [synth.from_spec(q) for q in reqs]
+    _engine_run(amber_b200, [synth.from_spec(dict(reqs[4], nn=64))], "mixed", dev)  # warm-up
+    with amber_b200.Estimator(device=dev, precision="mixed") as est:
+        eng = amber_b200.Engine(est)
+        p0 = eng.stats()["products"]
+        t0 = time.perf_counter()
+        tickets = []
+        for q, r in zip(reqs, reals):
+            delay = (q["arrival"] - reqs[0]["arrival"]) - (time.perf_counter() - t0)
+            if delay > 0:
+                time.sleep(delay)
+            tickets.append(eng.enqueue(r, want_v2=True))
+        lat = [eng.result(t, r, want_v2=True)[4] for t, r in zip(tickets, reals)]
+        wall = time.perf_counter() - t0
+        st = eng.stats()
+        prod = st["products"] - p0
+    small = sorted(range(n), key=lambda i: reqs[i]["nn"] ** 2 * reqs[i]["nc"] * reqs[i]["nbins"])[:2]
+    f_prod, f_wall, f_lat = 0.0, 0.0, []
+    for i in small:
+        with amber_b200.Estimator(device=dev, precision="fp64") as e64:
+            t = time.perf_counter()
+            amber_b200.estimate(reals[i], precision="fp64", version=2, est=e64)
+            f_lat.append(1e3 * (time.perf_counter() - t))
+            f_prod += e64.last_run_stats()[0]
+            f_wall += time.perf_counter() - t
+    return {"workload": f"serving: first {n} requests of the Poisson stream (50 req/s), sides/channels/bins as drawn",
+            "requests": n, "value": prod / wall, "unit": UNIT, "products": prod, "wall_s": wall,
+            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "latency_ms": [round(x, 1) for x in lat],
+            "engine": {k: st[k] for k in ("rounds", "contraction_launches", "max_active", "peak_bytes")},
+            "fp64_one_at_a_time": {"requests": small, "value": f_prod / f_wall, "latency_ms": f_lat,
+                                   "sizes": [(reqs[i]["nn"], reqs[i]["nc"], reqs[i]["nbins"]) for i in small]}}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -172,6 +262,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--tri-subset", default="", help="comma-separated triangle indices (profiling runs only)")
+    ap.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble measurement")
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving-stream measurement")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -355,9 +447,19 @@ def main():
                    "p50_ms": float(np.percentile(lat_ms, 50)), "p99_ms": float(np.percentile(lat_ms, 99))},
            "fp64_plain": fp64, "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
            "gpu_launches": int(launches), "products_per_step": products / args.steps}
+    est.close()
+    # batched ensemble and serving stream: 1 GPU only (the scaling runs measure the step above)
+    if rank == 0 and world == 1 and not args.tri_subset:
+        for key, flag, fn in (("ensemble", args.no_ensemble, ensemble_section),
+                              ("serving", args.no_serving, serving_section)):
+            if flag:
+                continue
+            try:
+                out[key] = fn(amber_b200, synth, local)
+            except Exception as ex:  # reported, not fatal
+                out[key] = {"error": str(ex)[:300]}
     if rank == 0:
         print(json.dumps(out))
-    est.close()
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()

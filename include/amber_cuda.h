@@ -190,7 +190,11 @@ typedef struct amber_cuda_engine_info {
     size_t peak_bytes;         /* most footprint admitted at once */
     size_t budget_bytes;       /* the engine's share of the context budget */
     double products;           /* lag-triple products of the finished requests */
-    double busy_ms;            /* wall time spent in rounds */
+    double busy_ms;            /* wall time spent in rounds, split into: */
+    double setup_ms;           /*   cube upload, rings, channels and calCR of newly admitted requests */
+    double maps_ms;            /*   ring-map batches */
+    double contract_ms;        /*   contractions and lag reductions */
+    double finish_ms;          /*   results back to the host, child contexts freed */
 } amber_cuda_engine_info;
 
 AMBER_API int amber_cuda_enqueue(amber_cuda_ctx *ctx, const amber_cuda_request *req, int64_t *ticket);
