@@ -76,10 +76,13 @@ int twiddle_table(amber_cuda_ctx *c, long n, const double2 **out)
     auto it = c->twiddles.find(n);
     if (it == c->twiddles.end()) {
         std::vector<double2> h(n);
-        for (long k = 0; k < n; ++k) {
+        for (long k = 0; k <= n / 2; ++k) {
             long double a = 2.0L * 3.14159265358979323846264338327950288L * (long double)k / (long double)n;
             h[k] = make_double2((double)cosl(a), (double)sinl(a));
         }
+        // exactly conjugate-symmetric, e^{2πi(n−k)/n} = conj(e^{2πik/n}): the map builder
+        // evaluates pixels x and n − x from one twiddle
+        for (long k = n / 2 + 1; k < n; ++k) h[k] = make_double2(h[n - k].x, -h[n - k].y);
         DevBuf b;
         int rc = ensure(c, b, sizeof(double2) * n, "twiddle table");
         if (rc) return rc;

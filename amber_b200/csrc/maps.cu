@@ -22,7 +22,9 @@
 // shared memory together with the twiddle table e^{2πik/Ng1}; lanes of a warp
 // walk channels (coalesced loads of the channel-innermost grid and of Y) and
 // share one twiddle per step (a shared-memory broadcast).  Twiddle indices
-// advance incrementally (k += n mod Ng1), so the inner loop is FP64 FMA work.
+// advance incrementally (k += n mod Ng1), so the inner loop is FP64 FMA work;
+// pass 2 evaluates pixels n1 and Ng1 − n1 from the same twiddle (the table is
+// exactly conjugate-symmetric).
 // All arithmetic is FP64.
 #include <cuda_bf16.h>
 #include <math.h>
@@ -197,21 +199,26 @@ __global__ void __launch_bounds__(kThreads) ring_rows_kernel(const double2 *__re
     __syncthreads();
 
     constexpr int G = 32 / C;
-    constexpr int R = 8;
+    // A thread evaluates R pixel pairs (x, Ng − x): they share each twiddle, cos and −sin,
+    // so one shared-memory load and one index step feed four FMAs.  x runs over [0, Ng/2];
+    // for x = 0 and x = Ng/2 the pair is one pixel.
+    constexpr int R = 4;
     const int q = lane % C, g = lane / C;
     const int gid = warp * G + g;
     const int ngroups = (kThreads / 32) * G;
+    const long npair = ng / 2 + 1;
     const long slot_row = ((long)s * nch + q0 + q) * kp + n0 * ng;
     float amax = 0.f;  // max |fp32 value| this thread writes (row exponent for the int8 digits)
-    for (long nb = gid; nb * R < ng; nb += ngroups) {
-        double acc[R];
+    for (long nb = gid; nb * R < npair; nb += ngroups) {
+        double acc[R], accm[R];  // pixel x, pixel Ng − x
         int idx[R], step[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-            long n1 = nb * R + r;
-            step[r] = (int)(n1 < ng ? n1 : 0);
+            long x = nb * R + r;
+            step[r] = (int)(x < npair ? x : 0);
             idx[r] = 0;
             acc[r] = 0.0;
+            accm[r] = 0.0;
         }
         for (int jj = 0; jj < J; ++jj) {
             double2 y = ys[jj * C + q];
@@ -220,6 +227,8 @@ __global__ void __launch_bounds__(kThreads) ring_rows_kernel(const double2 *__re
                 double2 w = tw[idx[r]];
                 acc[r] = fma(y.x, w.x, acc[r]);
                 acc[r] = fma(-y.y, w.y, acc[r]);
+                accm[r] = fma(y.x, w.x, accm[r]);
+                accm[r] = fma(y.y, w.y, accm[r]);
                 int t = idx[r] + step[r];
                 idx[r] = t >= ng ? t - (int)ng : t;
             }
@@ -227,23 +236,28 @@ __global__ void __launch_bounds__(kThreads) ring_rows_kernel(const double2 *__re
         if (q0 + q < nch) {
 #pragma unroll
             for (int r = 0; r < R; ++r) {
-                long n1 = nb * R + r;
-                if (n1 >= ng) continue;
-                long o = slot_row + n1;
-                double v = acc[r];
-                if (out_f64) out_f64[o] = v;
-                if (out_f32) {
-                    float f = (float)v;
-                    out_f32[o] = f;
-                    amax = fmaxf(amax, fabsf(f));
-                }
-                if (out_hi) {
-                    // split: hi = bf16(v), lo = bf16(v − hi) (both round-to-nearest)
-                    float f = (float)v;
-                    uint16_t h = bf16_bits(f);
-                    float hf = __uint_as_float((uint32_t)h << 16);
-                    out_hi[o] = h;
-                    out_lo[o] = bf16_bits((float)(v - (double)hf));
+                const long x = nb * R + r;
+                if (x >= npair) continue;
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const long n1 = h == 0 ? x : ng - x;
+                    if (h == 1 && (x == 0 || n1 == x)) continue;
+                    const long o = slot_row + n1;
+                    const double v = h == 0 ? acc[r] : accm[r];
+                    if (out_f64) out_f64[o] = v;
+                    if (out_f32) {
+                        float f = (float)v;
+                        out_f32[o] = f;
+                        amax = fmaxf(amax, fabsf(f));
+                    }
+                    if (out_hi) {
+                        // split: hi = bf16(v), lo = bf16(v − hi) (both round-to-nearest)
+                        float f = (float)v;
+                        uint16_t hb = bf16_bits(f);
+                        float hf = __uint_as_float((uint32_t)hb << 16);
+                        out_hi[o] = hb;
+                        out_lo[o] = bf16_bits((float)(v - (double)hf));
+                    }
                 }
             }
         }
