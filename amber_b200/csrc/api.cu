@@ -281,7 +281,9 @@ int run_next_batch(amber_cuda_ctx *c, RunState &st, std::vector<I8Job> *jobs)
     // The next batch of the group: triangles whose ring union fits the budget.
     size_t spare = c->budget > c->held ? c->budget - c->held : 0;
     spare += c->maps_d.bytes + c->maps_i.bytes + c->y.bytes;
-    const size_t reserve = (size_t)64 << 20;
+    // keep room for the mixed-precision contraction's partial tiles when they live in this context
+    const size_t reserve = ((size_t)64 << 20) +
+                           (prec == AMBER_PREC_MIXED && !c->contracts_elsewhere ? contract_partial_cap(c) : 0);
     const long cap_slots = (long)((spare > reserve ? spare - reserve : 0) /
                                   (map_slot_bytes(prec, g.ng, c->nc, want_v2) + 1));
     if (cap_slots < 3) return fail(c, AMBER_ERR_OOM, "maps of one triangle (Ng1=%ld) exceed the budget", g.ng);

@@ -82,6 +82,7 @@ struct amber_cuda_ctx {
     void *stage = nullptr; // pinned host staging of the job descriptors
     size_t stage_bytes = 0;
     amber::Engine *engine = nullptr;  // batched requests, created on the first enqueue
+    bool contracts_elsewhere = false; // an engine's child context: its jobs run in the owner's contraction
 
     // per-phase device timing of the last run (CUDA events on the launch stream)
     struct PhaseEv {
@@ -192,8 +193,11 @@ long ring_ng1(double uhigh, double du);
 std::vector<int> closed_triangles(const std::vector<double> &ulow, const std::vector<double> &uhigh);
 // Stops the context's request engine (pending requests finish, queued ones are dropped).
 void engine_shutdown(amber_cuda_ctx *c);
-// lag[d] = Σ_u partial[u][d] (compensated, fixed order).
-int lag_reduce(amber_cuda_ctx *c, const double *partial, long nunits, long ncsize, double *lag);
+// lag[d] = Σ_u partial[u][d] (compensated, fixed order); accumulate adds to lag[d].
+int lag_reduce(amber_cuda_ctx *c, const double *partial, long nunits, long ncsize, double *lag,
+               bool accumulate = false);
+// Device bytes the mixed-precision contraction keeps for the partial tiles of one launch.
+size_t contract_partial_cap(const amber_cuda_ctx *c);
 // Σ_x a·b·c over n points (FP64, deterministic) into out[0].
 int triple_sum(amber_cuda_ctx *c, const double *a, const double *b, const double *cc, long n, double *out);
 

@@ -155,12 +155,14 @@ __global__ void lag_reduce_groups(const double *__restrict__ partial, long nunit
     part[(long)(G + g) * ncsize + d] = comp;
 }
 
-// Pass 2: lag[d] = the groups' sums added in group order (TwoSum again) plus all compensations.
-__global__ void lag_reduce_final(const double *__restrict__ part, int G, long ncsize, double *__restrict__ lag)
+// Pass 2: lag[d] = the groups' sums added in group order (TwoSum again) plus all compensations;
+// with accumulate, the sum starts from the lag array's current value (a job split into anchor groups).
+__global__ void lag_reduce_final(const double *__restrict__ part, int G, long ncsize, int accumulate,
+                                 double *__restrict__ lag)
 {
     const long d = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (d >= ncsize) return;
-    double s = 0.0, comp = 0.0;
+    double s = accumulate ? lag[d] : 0.0, comp = 0.0;
     for (int g = 0; g < G; ++g) {
         const double v = part[(long)g * ncsize + d];
         const double t = s + v;
@@ -203,7 +205,7 @@ __global__ void sum_fixed(const double *__restrict__ part, int n, double *__rest
 
 }  // namespace
 
-int lag_reduce(amber_cuda_ctx *c, const double *partial, long nunits, long ncsize, double *lag)
+int lag_reduce(amber_cuda_ctx *c, const double *partial, long nunits, long ncsize, double *lag, bool accumulate)
 {
     // enough unit groups to give every SM several blocks; the grouping depends only on
     // (nunits, ncsize, SM count), so the result is deterministic
@@ -214,7 +216,7 @@ int lag_reduce(amber_cuda_ctx *c, const double *partial, long nunits, long ncsiz
     double *part = (double *)c->lagred.p;
     phase_begin(c, 2);
     lag_reduce_groups<<<dim3((unsigned)bx, (unsigned)G), 256, 0, c->stream>>>(partial, nunits, ncsize, part);
-    lag_reduce_final<<<(unsigned)bx, 256, 0, c->stream>>>(part, (int)G, ncsize, lag);
+    lag_reduce_final<<<(unsigned)bx, 256, 0, c->stream>>>(part, (int)G, ncsize, accumulate ? 1 : 0, lag);
     phase_end(c);
     c->launches += 2;
     return cuda_check(c, cudaGetLastError(), "lag reduction launch");

@@ -57,6 +57,7 @@
 // host turns into AMBER_ERR_TIMEOUT, drains its own copies and MMAs, frees TMEM.
 #include <algorithm>
 #include <cmath>
+#include <deque>
 #include <vector>
 
 #include "common.cuh"
@@ -572,6 +573,7 @@ struct Planned {
     int bn, mt, nt;
     long nch, chunk;
     size_t partial_bytes;
+    bool accumulate;  // a later anchor group of a split job: its lag sum adds to the array
 };
 
 template <int BN>
@@ -633,6 +635,11 @@ int fill_launch(amber_cuda_ctx *c, LaunchPlan &lp, char *stage)
 
 }  // namespace
 
+size_t contract_partial_cap(const amber_cuda_ctx *c)
+{
+    return std::max<size_t>((size_t)512 << 20, std::min<size_t>((size_t)8 << 30, c->budget / 8));
+}
+
 int contract_i8_jobs(amber_cuda_ctx *c, const std::vector<I8Job> &jobs)
 {
     int rc;
@@ -647,9 +654,10 @@ int contract_i8_jobs(amber_cuda_ctx *c, const std::vector<I8Job> &jobs)
     // jobs share persistent launches (one CTA per SM looping over the list), so a batch
     // of them fills the GPU without a tail per job.  Partial tiles of one launch stay
     // within a slice of the budget.
-    const size_t pcap = std::max<size_t>((size_t)512 << 20, std::min<size_t>((size_t)8 << 30, c->budget / 8));
+    const size_t pcap = contract_partial_cap(c);
     const long big_items = 4L * c->num_sms;
     std::vector<LaunchPlan> plans;
+    std::deque<I8Job> parts;  // anchor groups of jobs whose partial tiles exceed the cap
     for (int BN : {32, 64}) {
         LaunchPlan shared;
         for (const I8Job &jb : jobs) {
@@ -670,6 +678,30 @@ int contract_i8_jobs(amber_cuda_ctx *c, const std::vector<I8Job> &jobs)
             p.chunk = ((jb.k + p.nch - 1) / p.nch + KB_B - 1) / KB_B * KB_B;
             p.nch = (jb.k + p.chunk - 1) / p.chunk;
             p.partial_bytes = (sizeof(double) * (size_t)jb.nanchors * p.nch * ncsize + 255) / 256 * 256;
+            p.accumulate = false;
+            if (p.partial_bytes > pcap) {
+                // split the anchors into groups whose partial tiles fit; each group is a launch of
+                // its own and adds its sum to the lag array in group order (deterministic)
+                const long ng = (long)((p.partial_bytes + pcap - 1) / pcap);
+                const long per = (jb.nanchors + ng - 1) / ng;
+                for (long a0 = 0; a0 < jb.nanchors; a0 += per) {
+                    parts.push_back(jb);
+                    I8Job &sj = parts.back();
+                    sj.anchors = jb.anchors + a0;
+                    sj.nanchors = (int)std::min<long>(per, jb.nanchors - a0);
+                    Planned q = p;
+                    q.job = &sj;
+                    q.accumulate = a0 > 0;
+                    q.partial_bytes = (sizeof(double) * (size_t)sj.nanchors * q.nch * ncsize + 255) / 256 * 256;
+                    LaunchPlan lp;
+                    lp.persistent = false;
+                    lp.jobs.push_back(q);
+                    lp.nitems = (long)sj.nanchors * q.mt * q.nt * q.nch;
+                    lp.partial_bytes = q.partial_bytes;
+                    plans.push_back(lp);
+                }
+                continue;
+            }
             const long ni = (long)jb.nanchors * p.mt * p.nt * p.nch;
             if (ni >= big_items) {
                 LaunchPlan lp;
@@ -730,7 +762,8 @@ int contract_i8_jobs(amber_cuda_ctx *c, const std::vector<I8Job> &jobs)
         for (size_t i = 0; i < lp.jobs.size(); ++i) {
             const I8Job &jb = *lp.jobs[i].job;
             const long ncsize = (long)(2 * jb.nc10 + 1) * (2 * jb.nc10 + 1);
-            if ((rc = lag_reduce(c, h_desc[i].partial, (long)jb.nanchors * lp.jobs[i].nch, ncsize, jb.lag_out)))
+            if ((rc = lag_reduce(c, h_desc[i].partial, (long)jb.nanchors * lp.jobs[i].nch, ncsize, jb.lag_out,
+                                 lp.jobs[i].accumulate)))
                 return rc;
         }
     }

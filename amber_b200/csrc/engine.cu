@@ -169,6 +169,7 @@ int Engine::setup(Request *r)
     int rc = amber_cuda_create(&o, &r->sub);
     if (rc) return rc;
     amber_cuda_ctx *s = r->sub;
+    s->contracts_elsewhere = owner->precision == AMBER_PREC_MIXED;
     if ((rc = amber_cuda_load_grid_packed(s, r->N1, r->nc, r->Du, r->flag_key, r->re_im.data(), r->ntig.data())))
         return rc;
     // the host copies are no longer needed once the cube is on the device

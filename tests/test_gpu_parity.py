@@ -114,6 +114,30 @@ def test_mixed_vs_fp64_full_size(lib_built):
     assert ei.max() <= TOL["mixed"], (sample[int(ei.argmax())], ei.max())
 
 
+def test_split_anchor_groups_match(lib_built):
+    """A job whose partial tiles exceed the per-launch cap runs as anchor groups whose lag sums add
+    up in order.  128-pixel chunks on the Ng1 = 354 triangle of the single-realisation workload
+    make its partial tiles ~14 GB (the cap is at most 8 GB): the result must equal the default
+    chunking's up to the FP64 summation order."""
+    import amber_b200
+    real = synth.config2(seed=1)
+    out = []
+    for chunk_px in (0, 128):
+        with amber_b200.Estimator(precision="mixed", chunk_px=chunk_px) as est:
+            est.load_grid(real.gv, real.counts, real.du, real.flag_key)
+            est.set_rings(real.ulow, real.uhigh)
+            est.set_channels(real.nc10, real.uf_chans)
+            tri = est.calcr()[:, :3].astype(np.int32)
+            est.run(tri[[140]], want_v2=True)
+            out.append(est.fetch(want_v2=True))
+            n_launch = est.last_run_breakdown()[4]
+    (b0, n0, t0), (b1, n1, t1) = out
+    assert n_launch >= 4  # two anchor groups per pass
+    np.testing.assert_array_equal(n0, n1)
+    np.testing.assert_allclose(b1, b0, rtol=0, atol=1e-12 * np.abs(b0).max())
+    np.testing.assert_allclose(t1, t0, rtol=0, atol=1e-12 * np.abs(t0).max())
+
+
 def test_triangle_v1_v2_file_scalars(lib_built):
     import amber_b200
     z = np.load(os.path.join(GOLDEN, "est_flagged48.npz"))
