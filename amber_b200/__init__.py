@@ -38,6 +38,7 @@ EXPORTS = (
     "amber_cuda_triangle_v2", "amber_cuda_triangles", "amber_cuda_triangles_run", "amber_cuda_triangles_fetch",
     "amber_cuda_last_run_stats", "amber_cuda_last_run_breakdown", "amber_cuda_grid_vis",
     "amber_cuda_enqueue", "amber_cuda_wait", "amber_cuda_result", "amber_cuda_engine_stats",
+    "amber_cuda_tile_choices",
 )
 
 
@@ -68,7 +69,7 @@ class EngineInfo(ctypes.Structure):
 
 class Opts(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("precision", ctypes.c_int), ("hbm_budget", ctypes.c_size_t),
-                ("stream", ctypes.c_void_p), ("chunk_px", ctypes.c_int)]
+                ("stream", ctypes.c_void_p), ("chunk_px", ctypes.c_int), ("tile_n", ctypes.c_int)]
 
 
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -121,6 +122,7 @@ def load_library():
     L.amber_cuda_wait.argtypes = [_vp, ctypes.c_int64, ctypes.c_int, _ip]
     L.amber_cuda_result.argtypes = [_vp, ctypes.c_int64, ctypes.c_int, _dp, _dp, _i64p, _dp, _dp]
     L.amber_cuda_engine_stats.argtypes = [_vp, ctypes.POINTER(EngineInfo)]
+    L.amber_cuda_tile_choices.argtypes = [_vp, ctypes.c_int, _ip, _ip, _fp, _fp]
     _lib = L
     return L
 
@@ -133,9 +135,9 @@ class Estimator:
     """One libamber_cuda context (one device, one host thread)."""
 
     def __init__(self, device: int = 0, precision: str = "mixed", hbm_budget: int = 0, stream: int | None = None,
-                 chunk_px: int = 0):
+                 chunk_px: int = 0, tile_n: int = 0):
         self._L = load_library()
-        o = Opts(device, PREC[precision], hbm_budget, stream or None, chunk_px)
+        o = Opts(device, PREC[precision], hbm_budget, stream or None, chunk_px, tile_n)
         h = _vp()
         rc = self._L.amber_cuda_create(ctypes.byref(o), ctypes.byref(h))
         if rc != AMBER_OK:
@@ -266,6 +268,15 @@ class Estimator:
         p, ms = ctypes.c_double(), ctypes.c_double()
         self._check(self._L.amber_cuda_last_run_stats(self._h, ctypes.byref(p), ctypes.byref(ms)))
         return p.value, ms.value
+
+    def tile_choices(self) -> dict:
+        """Autotuner decisions: {nclen class: (tile width, trial ms at 32, at 64)} (0 when another context
+        of the process ran the trial)."""
+        n = self._L.amber_cuda_tile_choices(self._h, 0, None, None, None, None)
+        cls, bn = np.zeros(max(n, 1), np.int32), np.zeros(max(n, 1), np.int32)
+        t32, t64 = np.zeros(max(n, 1), np.float32), np.zeros(max(n, 1), np.float32)
+        self._L.amber_cuda_tile_choices(self._h, n, _ptr(cls, _ip), _ptr(bn, _ip), _ptr(t32, _fp), _ptr(t64, _fp))
+        return {int(cls[i]): (int(bn[i]), float(t32[i]), float(t64[i])) for i in range(n)}
 
     def last_run_breakdown(self):
         """(ms_maps, ms_contract, ms_reduce, kernel_launches, contract_launches) of the last run."""

@@ -447,6 +447,11 @@ int amber_cuda_create(const amber_cuda_opts *opts, amber_cuda_ctx **out)
     c->precision = o.precision == AMBER_PREC_FP64_ABS ? AMBER_PREC_FP64 : o.precision;
     c->fp64_abs = o.precision == AMBER_PREC_FP64_ABS;
     c->chunk_px = o.chunk_px;
+    if (o.tile_n != 0 && o.tile_n != 32 && o.tile_n != 64) {
+        delete c;
+        return AMBER_ERR_ARG;
+    }
+    c->tile_n = o.tile_n;
     c->num_sms = prop.multiProcessorCount;
     size_t fr = 0, tot = 0;
     cudaMemGetInfo(&fr, &tot);
@@ -459,6 +464,8 @@ int amber_cuda_create(const amber_cuda_opts *opts, amber_cuda_ctx **out)
     }
     cudaEventCreate(&c->ev0);
     cudaEventCreate(&c->ev1);
+    cudaEventCreate(&c->tev0);
+    cudaEventCreate(&c->tev1);
     *out = c;
     return AMBER_OK;
 }
@@ -470,7 +477,7 @@ void amber_cuda_destroy(amber_cuda_ctx *c)
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);
     DevBuf *bufs[] = {&c->grid, &c->mask, &c->d_weight, &c->d_anchors, &c->y, &c->maps_d, &c->maps_i,
-                      &c->partial, &c->results, &c->ring_lohi, &c->misc, &c->mixed_scratch, &c->lagred, &c->jobdesc};
+                      &c->partial, &c->results, &c->ring_lohi, &c->misc, &c->mixed_scratch, &c->lagred, &c->jobdesc, &c->lagtrial};
     for (DevBuf *b : bufs) release(c, *b);
     if (c->stage) cudaFreeHost(c->stage);
     c->stage = nullptr;
@@ -481,6 +488,8 @@ void amber_cuda_destroy(amber_cuda_ctx *c)
     }
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->tev0) cudaEventDestroy(c->tev0);
+    if (c->tev1) cudaEventDestroy(c->tev1);
     if (c->own_stream) cudaStreamDestroy(c->stream);
     delete c;
 }
@@ -721,6 +730,25 @@ int amber_cuda_triangles(amber_cuda_ctx *c, int ntri, const int *tri, int want_v
     int rc = amber_cuda_triangles_run(c, ntri, tri, want_v2);
     if (rc) return rc;
     return amber_cuda_triangles_fetch(c, bldnu, numdnu, numtri);
+}
+
+int amber_cuda_tile_choices(const amber_cuda_ctx *c, int max_entries, int *nclen_class, int *tile_n,
+                            float *ms_trial_32, float *ms_trial_64)
+{
+    if (!c || max_entries < 0) return AMBER_ERR_ARG;
+    int n = 0;
+    for (const auto &kv : c->tile_tuned) {
+        if (n < max_entries) {
+            if (nclen_class) nclen_class[n] = kv.first;
+            if (tile_n) tile_n[n] = kv.second;
+            for (const auto &t : c->tile_trials) {
+                if (t.first == kv.first * 100 + 32 && ms_trial_32) ms_trial_32[n] = t.second;
+                if (t.first == kv.first * 100 + 64 && ms_trial_64) ms_trial_64[n] = t.second;
+            }
+        }
+        ++n;
+    }
+    return n;
 }
 
 int amber_cuda_last_run_stats(const amber_cuda_ctx *c, double *products, double *device_ms)

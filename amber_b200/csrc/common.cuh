@@ -42,6 +42,9 @@ struct amber_cuda_ctx {
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     int chunk_px = 0;
+    int tile_n = 0;                // mixed path: forced p3 tile width, 0 = autotuned
+    std::map<int, int> tile_tuned; // autotuner: lag-window class (nclen rounded up to 8) → p3 tile width
+    std::vector<std::pair<int, float>> tile_trials;  // autotuner trials run here: (class·100 + BN, ms)
     int num_sms = 148;
     std::string err;
 
@@ -79,6 +82,7 @@ struct amber_cuda_ctx {
     amber::DevBuf mixed_scratch;
     amber::DevBuf lagred;  // two-pass lag reduction: per-group sums and compensations
     amber::DevBuf jobdesc; // contraction job descriptors and work items
+    amber::DevBuf lagtrial; // autotuner: lag array of a discarded trial run
     void *stage = nullptr; // pinned host staging of the job descriptors
     size_t stage_bytes = 0;
     amber::Engine *engine = nullptr;  // batched requests, created on the first enqueue
@@ -102,6 +106,7 @@ struct amber_cuda_ctx {
     double last_products = 0;
     float last_ms = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t tev0 = nullptr, tev1 = nullptr;  // autotuner trials
 };
 
 namespace amber {

@@ -58,6 +58,8 @@
 #include <algorithm>
 #include <cmath>
 #include <deque>
+#include <map>
+#include <mutex>
 #include <vector>
 
 #include "common.cuh"
@@ -597,7 +599,7 @@ struct LaunchPlan {
     bool persistent = true;  // false: one CTA per item, dispatched by the hardware as SMs free up
 };
 
-int fill_launch(amber_cuda_ctx *c, LaunchPlan &lp, char *stage)
+int fill_launch(amber_cuda_ctx *c, LaunchPlan &lp, char *stage, bool first_chunk_only)
 {
     int rc;
     const int BN = lp.jobs[0].bn;
@@ -626,7 +628,7 @@ int fill_launch(amber_cuda_ctx *c, LaunchPlan &lp, char *stage)
         d.k = jb.k; d.kp = jb.kp; d.chunk = p.chunk;
         d.nc = jb.nc; d.nc10 = jb.nc10; d.nclen = 2 * jb.nc10 + 1;
         d.mt_count = p.mt; d.nt_count = p.nt; d.nchunk = (int)p.nch; d.nanchors = jb.nanchors;
-        const long n_local = (long)jb.nanchors * p.mt * p.nt * p.nch;
+        const long n_local = (long)jb.nanchors * p.mt * p.nt * (first_chunk_only ? 1 : p.nch);
         for (long q = 0; q < n_local; ++q) items[ni++] = Item{(int)i, (int)q};
         poff += p.partial_bytes;
     }
@@ -640,12 +642,13 @@ size_t contract_partial_cap(const amber_cuda_ctx *c)
     return std::max<size_t>((size_t)512 << 20, std::min<size_t>((size_t)8 << 30, c->budget / 8));
 }
 
-int contract_i8_jobs(amber_cuda_ctx *c, const std::vector<I8Job> &jobs)
+namespace {
+
+// Plans and enqueues the launches of a list of jobs, job i with p3 tile width bn[i].
+int execute_jobs(amber_cuda_ctx *c, const std::vector<const I8Job *> &jobs, const std::vector<int> &bn, int *d_err,
+                 bool first_chunk_only = false)
 {
     int rc;
-    if ((rc = ensure(c, c->misc, 256, "error flag"))) return rc;
-    int *d_err = (int *)c->misc.p;
-    if ((rc = cuda_check(c, cudaMemsetAsync(d_err, 0, sizeof(int), c->stream), "error flag"))) return rc;
     long max_chunk = c->chunk_px > 0 ? std::min<long>(c->chunk_px, 32768) : 32768;
     max_chunk = std::max<long>(KB_B, max_chunk / KB_B * KB_B);
     // Launch plan.  A job with many items runs in a launch of its own with one CTA per
@@ -660,10 +663,11 @@ int contract_i8_jobs(amber_cuda_ctx *c, const std::vector<I8Job> &jobs)
     std::deque<I8Job> parts;  // anchor groups of jobs whose partial tiles exceed the cap
     for (int BN : {32, 64}) {
         LaunchPlan shared;
-        for (const I8Job &jb : jobs) {
+        for (size_t ji = 0; ji < jobs.size(); ++ji) {
+            const I8Job &jb = *jobs[ji];
             const int nclen = 2 * jb.nc10 + 1;
             const long ncsize = (long)nclen * nclen;
-            if ((nclen <= 32 ? 32 : 64) != BN) continue;
+            if (bn[ji] != BN) continue;
             if (jb.nanchors == 0) {
                 if ((rc = cuda_check(c, cudaMemsetAsync(jb.lag_out, 0, sizeof(double) * ncsize, c->stream), "zero lag")))
                     return rc;
@@ -674,7 +678,9 @@ int contract_i8_jobs(amber_cuda_ctx *c, const std::vector<I8Job> &jobs)
             p.bn = BN;
             p.mt = (nclen + BM - 1) / BM;
             p.nt = (nclen + BN - 1) / BN;
-            p.nch = choose_chunks(jb.k, (long)jb.nanchors * p.mt * p.nt, c->num_sms, ncsize, max_chunk);
+            // the chunk count (and with it the FP64 summation grouping) must not depend on BN, so
+            // that the tile width is numerically neutral: it is planned for 64-wide tiles
+            p.nch = choose_chunks(jb.k, (long)jb.nanchors * p.mt * ((nclen + 63) / 64), c->num_sms, ncsize, max_chunk);
             p.chunk = ((jb.k + p.nch - 1) / p.nch + KB_B - 1) / KB_B * KB_B;
             p.nch = (jb.k + p.chunk - 1) / p.chunk;
             p.partial_bytes = (sizeof(double) * (size_t)jb.nanchors * p.nch * ncsize + 255) / 256 * 256;
@@ -744,8 +750,13 @@ int contract_i8_jobs(amber_cuda_ctx *c, const std::vector<I8Job> &jobs)
     }
     // the staging area may still feed the previous run's upload
     if ((rc = cuda_check(c, cudaStreamSynchronize(c->stream), "job staging"))) return rc;
+    if (first_chunk_only)
+        for (LaunchPlan &lp : plans) {
+            lp.nitems = 0;
+            for (const Planned &p : lp.jobs) lp.nitems += (long)p.job->nanchors * p.mt * p.nt;
+        }
     for (LaunchPlan &lp : plans)
-        if ((rc = fill_launch(c, lp, (char *)c->stage))) return rc;
+        if ((rc = fill_launch(c, lp, (char *)c->stage, first_chunk_only))) return rc;
     if ((rc = cuda_check(c, cudaMemcpyAsync(c->jobdesc.p, c->stage, stage_bytes, cudaMemcpyHostToDevice, c->stream),
                          "job list upload")))
         return rc;
@@ -758,6 +769,7 @@ int contract_i8_jobs(amber_cuda_ctx *c, const std::vector<I8Job> &jobs)
                                  : launch<64>(c, d_jobs, d_items, lp.nitems, grid, d_err);
         phase_end(c);
         if (rc) return rc;
+        if (first_chunk_only) continue;  // a timing trial: its partial tiles are not reduced
         const JobDesc *h_desc = (const JobDesc *)((char *)c->stage + lp.desc_off);
         for (size_t i = 0; i < lp.jobs.size(); ++i) {
             const I8Job &jb = *lp.jobs[i].job;
@@ -767,6 +779,83 @@ int contract_i8_jobs(amber_cuda_ctx *c, const std::vector<I8Job> &jobs)
                 return rc;
         }
     }
+    return AMBER_OK;
+}
+
+// Lag-window class of the autotuner: nclen rounded up to 8.
+int tile_class(int nclen) { return (nclen + 7) / 8 * 8; }
+
+// The autotuner's decisions, per (device, class), shared by every context of the process:
+// the choice never changes a result, only the time.
+std::mutex g_tile_mu;
+std::map<std::pair<int, int>, int> g_tile_choice;
+
+}  // namespace
+
+int contract_i8_jobs(amber_cuda_ctx *c, const std::vector<I8Job> &jobs)
+{
+    int rc;
+    if ((rc = ensure(c, c->misc, 256, "error flag"))) return rc;
+    int *d_err = (int *)c->misc.p;
+    if ((rc = cuda_check(c, cudaMemsetAsync(d_err, 0, sizeof(int), c->stream), "error flag"))) return rc;
+    // Tile width: 32 for nclen ≤ 32, 64 above 128; in between both are possible (one 64-wide
+    // tile with idle columns, or more 32-wide tiles that each reload the A operand) and the
+    // autotuner measures the first job of each lag-window class with both, once per context.
+    // The int8 digit products accumulate exactly and the chunking does not depend on the tile
+    // width, so the choice does not change any result.
+    std::vector<const I8Job *> rest;
+    std::vector<int> bn;
+    for (const I8Job &jb : jobs) {
+        const int nclen = 2 * jb.nc10 + 1;
+        int w = nclen <= 32 ? 32 : 64;
+        if (c->tile_n && nclen <= 128) w = nclen <= 32 ? 32 : c->tile_n;
+        if (!c->tile_n && nclen > 32 && nclen <= 128 && jb.nanchors > 0) {
+            const int cls = tile_class(nclen);
+            int known = 0;
+            {
+                std::lock_guard<std::mutex> lk(g_tile_mu);
+                auto it = g_tile_choice.find({c->device, cls});
+                if (it != g_tile_choice.end()) known = it->second;
+            }
+            if (!known) {
+                // trial: the first pixel chunk of the job with both widths, each launch alone
+                // and timed; the job itself then runs with the winner below
+                const long ncsize = (long)nclen * nclen;
+                if ((rc = ensure(c, c->lagtrial, sizeof(double) * ncsize, "tile trial lag array"))) return rc;
+                I8Job scratch = jb;
+                scratch.lag_out = (double *)c->lagtrial.p;
+                // Each width alone, alternating, until both have been timed for at least 1.5 ms
+                // (at most 8 rounds), so that launch overhead and noise do not decide; 32 wins
+                // only when clearly (5 %) faster, otherwise the 64-wide default stays.
+                double tot[2] = {0, 0};
+                int reps = 0;
+                const int widths[2] = {32, 64};
+                while (reps < 8 && (reps < 2 || std::min(tot[0], tot[1]) < 1.5)) {
+                    for (int q0 = 0; q0 < 2; ++q0) {
+                        const int q = (reps & 1) ? 1 - q0 : q0;
+                        float ms = 0;
+                        cudaEventRecord(c->tev0, c->stream);
+                        if ((rc = execute_jobs(c, {&scratch}, {widths[q]}, d_err, true))) return rc;
+                        cudaEventRecord(c->tev1, c->stream);
+                        if ((rc = cuda_check(c, cudaEventSynchronize(c->tev1), "tile trial"))) return rc;
+                        cudaEventElapsedTime(&ms, c->tev0, c->tev1);
+                        tot[q] += ms;
+                    }
+                    ++reps;
+                }
+                c->tile_trials.push_back({cls * 100 + 32, (float)(tot[0] / reps)});
+                c->tile_trials.push_back({cls * 100 + 64, (float)(tot[1] / reps)});
+                known = tot[0] < 0.95 * tot[1] ? 32 : 64;
+                std::lock_guard<std::mutex> lk(g_tile_mu);
+                g_tile_choice[{c->device, cls}] = known;
+            }
+            c->tile_tuned[cls] = known;
+            w = known;
+        }
+        rest.push_back(&jb);
+        bn.push_back(w);
+    }
+    if (!rest.empty() && (rc = execute_jobs(c, rest, bn, d_err))) return rc;
     int herr = 0;
     if ((rc = cuda_check(c, cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream),
                          "error flag read")))

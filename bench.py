@@ -496,6 +496,8 @@ def main():
                    "p50_ms": float(np.percentile(lat_ms, 50)), "p99_ms": float(np.percentile(lat_ms, 99))},
            "fp64_plain": fp64, "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
            "gpu_launches": int(launches), "products_per_step": products / args.steps}
+    out["autotuner"] = {f"nclen<={k}": {"tile_n": v[0], "trial_ms_32": round(v[1], 3), "trial_ms_64": round(v[2], 3)}
+                        for k, v in est.tile_choices().items()}
     est.close()
     # batched ensemble and serving stream: 1 GPU only (the scaling runs measure the step above)
     if rank == 0 and world == 1 and not args.tri_subset:

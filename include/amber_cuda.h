@@ -54,6 +54,8 @@ typedef struct amber_cuda_opts {
     size_t hbm_budget;     /* max device bytes the context may hold; 0 = 90 % of free memory */
     void *stream;          /* optional cudaStream_t to launch on (NULL = the context's own stream) */
     int chunk_px;          /* tensor-core paths: pixels per CTA accumulation chunk before the FP64 flush (0 = default) */
+    int tile_n;            /* mixed path: p3 tile width 32 or 64; 0 = chosen by the autotuner (measured once per
+                              lag-window class and context).  Results do not depend on it. */
 } amber_cuda_opts;
 
 AMBER_API void amber_cuda_default_opts(amber_cuda_opts *opts);
@@ -131,6 +133,15 @@ AMBER_API int amber_cuda_last_run_stats(const amber_cuda_ctx *ctx, double *produ
  * reference times only the whole loop (amber.c:230,285). */
 AMBER_API int amber_cuda_last_run_breakdown(const amber_cuda_ctx *ctx, double *ms_maps, double *ms_contract,
                                             double *ms_reduce, long *kernel_launches, long *contract_launches);
+
+/* The autotuner's decisions seen by this context (mixed path, tile_n = 0): for each
+ * lag-window class (nclen rounded up to 8) the chosen p3 tile width and, where this
+ * context ran the trial, the two trials' times in ms (the first pixel chunk of one job,
+ * each width alone; decisions are shared by all contexts of the process on a device).
+ * Returns the number of classes (entries beyond max_entries are counted, not written).
+ * No reference counterpart. */
+AMBER_API int amber_cuda_tile_choices(const amber_cuda_ctx *ctx, int max_entries, int *nclen_class, int *tile_n,
+                                      float *ms_trial_32, float *ms_trial_64);
 
 /* ---- gridding: replaces group_loop_gridding / _without_flag
  * (3_vcg/tgefuncs.c:377-505, 511-621).  randpar[g·npar + {0,1}] = u/ν0, v/ν0

@@ -138,6 +138,25 @@ def test_split_anchor_groups_match(lib_built):
     np.testing.assert_allclose(t1, t0, rtol=0, atol=1e-12 * np.abs(t0).max())
 
 
+def test_tile_width_is_numerically_neutral(lib_built):
+    """The autotuner may pick either p3 tile width for 32 < nclen <= 128: the int8 digit products
+    accumulate exactly and the chunking is planned independently of the width, so forced 32,
+    forced 64 and the tuned choice give bit-identical lag arrays."""
+    import amber_b200
+    real = synth.tiny(64, 40, seed=52, nbins=6, hi=28.0, nc10=19, flagged=[0, 39])
+    outs = []
+    for tile_n in (32, 64, 0):
+        with amber_b200.Estimator(precision="mixed", tile_n=tile_n) as est:
+            amber_b200.estimate(real, precision="mixed", version=2, est=est)
+            outs.append(est.fetch(want_v2=True))
+            if tile_n == 0:
+                ch = est.tile_choices()
+    assert 40 in ch and ch[40][0] in (32, 64)
+    for o in outs[1:]:
+        for a, b in zip(outs[0], o):
+            np.testing.assert_array_equal(a, b)
+
+
 def test_triangle_v1_v2_file_scalars(lib_built):
     import amber_b200
     z = np.load(os.path.join(GOLDEN, "est_flagged48.npz"))
