@@ -36,9 +36,9 @@ EXPORTS = (
     "amber_cuda_load_grid_packed", "amber_cuda_load_grid", "amber_cuda_set_rings", "amber_cuda_get_uavg",
     "amber_cuda_set_channels", "amber_cuda_calcr", "amber_cuda_ng1", "amber_cuda_triangle_v1",
     "amber_cuda_triangle_v2", "amber_cuda_triangles", "amber_cuda_triangles_run", "amber_cuda_triangles_fetch",
-    "amber_cuda_last_run_stats", "amber_cuda_last_run_breakdown", "amber_cuda_grid_vis",
+    "amber_cuda_last_run_stats", "amber_cuda_last_run_breakdown", "amber_cuda_last_run_shape", "amber_cuda_grid_vis",
     "amber_cuda_enqueue", "amber_cuda_wait", "amber_cuda_result", "amber_cuda_engine_stats",
-    "amber_cuda_tile_choices",
+    "amber_cuda_tile_choices", "amber_cuda_cyl_bs",
 )
 
 
@@ -65,6 +65,23 @@ class EngineInfo(ctypes.Structure):
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class CylBsParams(ctypes.Structure):
+    _fields_ = [("n_cut", ctypes.c_int), ("window", ctypes.c_int), ("denominator", ctypes.c_int),
+                ("mabs_norm", ctypes.c_double), ("rc", ctypes.c_double), ("rc_prime", ctypes.c_double),
+                ("dnu_mhz", ctypes.c_double)]
+
+
+def reference_cylbs_constants():
+    """The analysis stage's constants (mabs_funcs.py:4-28), restated by the same formulas:
+    n_nancut, mabs_norm = fact·rjfac³ (beam solid angle × Jy→mK cubed), rc, rc_prime, dnu_mwa."""
+    import math
+    theta_0 = 0.6 * 24.68 * math.pi / 180
+    fact = math.pi * theta_0 * theta_0 / 3
+    nu0, k_b, c = 154.255e6, 1.38e3, 3e8
+    rjfac = 2.0 * k_b * nu0 * nu0 / (c * c) / 1e3
+    return dict(n_cut=8, mabs_norm=fact * rjfac ** 3, rc=9210.11291939594, rc_prime=17.0, dnu_mhz=0.04)
 
 
 class Opts(ctypes.Structure):
@@ -113,6 +130,7 @@ def load_library():
     L.amber_cuda_triangles_run.argtypes = [_vp, ctypes.c_int, _ip, ctypes.c_int]
     L.amber_cuda_triangles_fetch.argtypes = [_vp, _dp, _i64p, _dp]
     L.amber_cuda_last_run_stats.argtypes = [_vp, _dp, _dp]
+    L.amber_cuda_last_run_shape.argtypes = [_vp, _ip, _ip, _ip]
     L.amber_cuda_last_run_breakdown.argtypes = [_vp, _dp, _dp, _dp, ctypes.POINTER(ctypes.c_long),
                                                 ctypes.POINTER(ctypes.c_long)]
     L.amber_cuda_grid_vis.argtypes = [_vp, ctypes.c_long, ctypes.c_long, ctypes.c_double, ctypes.c_double,
@@ -123,6 +141,7 @@ def load_library():
     L.amber_cuda_result.argtypes = [_vp, ctypes.c_int64, ctypes.c_int, _dp, _dp, _i64p, _dp, _dp]
     L.amber_cuda_engine_stats.argtypes = [_vp, ctypes.POINTER(EngineInfo)]
     L.amber_cuda_tile_choices.argtypes = [_vp, ctypes.c_int, _ip, _ip, _fp, _fp]
+    L.amber_cuda_cyl_bs.argtypes = [_vp, ctypes.POINTER(CylBsParams), _dp, _dp]
     _lib = L
     return L
 
@@ -248,14 +267,19 @@ class Estimator:
 
     def run(self, tri, want_v2=False):
         tri = np.ascontiguousarray(np.asarray(tri, dtype=np.int32).reshape(-1, 3))
-        self._ntri = len(tri)
         self._check(self._L.amber_cuda_triangles_run(self._h, len(tri), _ptr(tri, _ip), int(bool(want_v2))))
 
+    def last_run_shape(self):
+        """(triangles, nclen, has v2 mask sums) of the results the last run left on the device."""
+        t, n, v = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        self._check(self._L.amber_cuda_last_run_shape(self._h, ctypes.byref(t), ctypes.byref(n), ctypes.byref(v)))
+        return t.value, n.value, bool(v.value)
+
     def fetch(self, want_v2=False):
-        n = self.nclen
-        bl = np.zeros((self._ntri, n, n))
-        nd = np.zeros((self._ntri, n, n), dtype=np.int64)
-        nt = np.zeros((self._ntri, n, n)) if want_v2 else None
+        ntri, n, _ = self.last_run_shape()
+        bl = np.zeros((ntri, n, n))
+        nd = np.zeros((ntri, n, n), dtype=np.int64)
+        nt = np.zeros((ntri, n, n)) if want_v2 else None
         self._check(self._L.amber_cuda_triangles_fetch(self._h, _ptr(bl, _dp), _ptr(nd, _i64p), _ptr(nt, _dp)))
         return bl, nd, nt
 
@@ -268,6 +292,26 @@ class Estimator:
         p, ms = ctypes.c_double(), ctypes.c_double()
         self._check(self._L.amber_cuda_last_run_stats(self._h, ctypes.byref(p), ctypes.byref(ms)))
         return p.value, ms.value
+
+    def cyl_bs(self, window=False, denominator="counts", tri_div=None, **const):
+        """Cylindrical bispectra [ntri, N, N] of the last run (amber_cuda_cyl_bs); ``denominator`` is
+        "counts" (v1) or "mask" (the sampling-mask sums of a v2 run); ``tri_div`` divides each
+        triangle's sums (Num for the v1 chain); constants default to the reference analysis stage's
+        (reference_cylbs_constants)."""
+        k = reference_cylbs_constants()
+        k.update(const)
+        p = CylBsParams(int(k["n_cut"]), int(bool(window)), 0 if denominator == "counts" else 1, float(k["mabs_norm"]),
+                        float(k["rc"]), float(k["rc_prime"]), float(k["dnu_mhz"]))
+        ntri, nclen, _ = self.last_run_shape()
+        n = max(nclen - 2 * int(k["n_cut"]), 1)
+        out = np.zeros((max(ntri, 1), n, n))
+        td = None
+        if tri_div is not None:
+            td = np.ascontiguousarray(tri_div, dtype=np.float64).reshape(-1)
+            if len(td) != ntri:
+                raise ValueError(f"tri_div has {len(td)} entries, the last run {ntri} triangles")
+        self._check(self._L.amber_cuda_cyl_bs(self._h, ctypes.byref(p), _ptr(td, _dp), _ptr(out, _dp)))
+        return out[:ntri]
 
     def tile_choices(self) -> dict:
         """Autotuner decisions: {nclen class: (tile width, trial ms at 32, at 64)} (0 when another context

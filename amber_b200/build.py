@@ -15,7 +15,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libamber_cuda.so")
 DRIVER = os.path.join(HERE, "amber_gpu")
-SOURCES = ["api.cu", "maps.cu", "contract64.cu", "contract_tc.cu", "contract_i8.cu", "grid.cu", "noalloc.cu", "engine.cu"]
+SOURCES = ["api.cu", "maps.cu", "contract64.cu", "contract_tc.cu", "contract_i8.cu", "grid.cu", "noalloc.cu", "engine.cu", "cylbs.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

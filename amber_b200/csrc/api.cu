@@ -595,6 +595,7 @@ int amber_cuda_set_channels(amber_cuda_ctx *c, int nc10, int uf_nc, const int *u
                          "anchors")))
         return rc;
     c->nc10 = nc10;
+    c->last_ntri = 0;  // the results buffer is laid out for the previous lag width
     c->uf.assign(uf_chans, uf_chans + uf_nc);
     c->weight = w;
     c->anchors = anchors;
@@ -645,6 +646,7 @@ int amber_cuda_calcr(amber_cuda_ctx *c, int max_tri, int *rcount, double *rdata)
                 }
     const int n = (int)tri.size() / 3;
     if ((rc = ensure(c, c->results, sizeof(double) * std::max(1, n), "calCR sums"))) return rc;
+    c->last_ntri = 0;  // the sums below overwrite the last triangle run's lag arrays
     const double *II = (const double *)c->maps_i.p;
     for (int t = 0; t < n; ++t)
         if ((rc = triple_sum(c, II + (long)tri[3 * t] * k, II + (long)tri[3 * t + 1] * k,
@@ -768,6 +770,15 @@ int amber_cuda_last_run_breakdown(const amber_cuda_ctx *c, double *ms_maps, doub
     if (ms_reduce) *ms_reduce = c->phase_ms[2];
     if (kernel_launches) *kernel_launches = c->launches;
     if (contract_launches) *contract_launches = c->contractions;
+    return AMBER_OK;
+}
+
+int amber_cuda_last_run_shape(const amber_cuda_ctx *c, int *ntri, int *nclen, int *v2)
+{
+    if (!c) return AMBER_ERR_ARG;
+    if (ntri) *ntri = c->last_ntri;
+    if (nclen) *nclen = 2 * c->nc10 + 1;
+    if (v2) *v2 = c->last_v2;
     return AMBER_OK;
 }
 

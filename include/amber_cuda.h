@@ -131,8 +131,38 @@ AMBER_API int amber_cuda_last_run_stats(const amber_cuda_ctx *ctx, double *produ
  * kernel and the lag reduction (CUDA events on the launch stream), and how
  * many of the library's kernels it launched.  No reference counterpart: the
  * reference times only the whole loop (amber.c:230,285). */
+/* Shape of the results the last amber_cuda_triangles_run left on the device
+ * (what _fetch and amber_cuda_cyl_bs read): its triangle count (0 once the
+ * channels are set again or calCR has reused the buffer), the lag width nclen
+ * and whether it holds the v2 mask sums. */
+AMBER_API int amber_cuda_last_run_shape(const amber_cuda_ctx *ctx, int *ntri, int *nclen, int *v2);
 AMBER_API int amber_cuda_last_run_breakdown(const amber_cuda_ctx *ctx, double *ms_maps, double *ms_contract,
                                             double *ms_reduce, long *kernel_launches, long *contract_launches);
+
+/* ---- cylindrical bispectrum: the analysis stage's lag→k step on the device.
+ * Replaces mabs_funcs.py get_cyl_BS (376-389: fold_quadrants 210-222, cut_nan
+ * 259-260, Bdnu2Bk_fft 325-334) and, with window = 1, mfunc_winds.py
+ * cylbs_win (122-136: mabs_win 88-103, blackman_nuttall 17-31), for every
+ * triangle of the last amber_cuda_triangles_run at once: fold the (Δ2, Δ3)
+ * quadrants, divide by mabs_norm and by the folded normaliser (denominator 0:
+ * the triplet counts, as in v1 files; 1: the sampling-mask sums of a v2 run,
+ * as in v2 files), cut n_cut cells at the edges, optionally window, then the
+ * shifted inverse real 2D transform scaled by rc⁴·(N·dnu_mhz·rc_prime)².
+ * tri_div (host, [ntri], may be NULL) divides each triangle's sums first: the v1
+ * reader returns bldnu / Num (mabs_funcs.py:172-187), so pass Num for that chain.
+ * out is [ntri][N][N] FP64 with N = 2·(nc10 + 1 − n_cut) − 1.  The reference
+ * reads the lag arrays back from float files; here they are the FP64 sums. */
+typedef struct amber_cuda_cylbs_params {
+    int n_cut;        /* edge cells cut after folding (mabs_funcs.py n_nancut = 8) */
+    int window;       /* 1: Blackman–Nuttall window, 0: none */
+    int denominator;  /* 0: triplet counts, 1: sampling-mask sums (v2 run) */
+    double mabs_norm; /* divisor of the folded sums (mabs_funcs.py fact·rjfac³) */
+    double rc;        /* comoving distance, Mpc (mabs_funcs.py rc) */
+    double rc_prime;  /* its derivative, Mpc/MHz (rc_prime) */
+    double dnu_mhz;   /* channel width, MHz (dnu_mwa) */
+} amber_cuda_cylbs_params;
+AMBER_API int amber_cuda_cyl_bs(amber_cuda_ctx *ctx, const amber_cuda_cylbs_params *p, const double *tri_div,
+                                double *out);
 
 /* The autotuner's decisions seen by this context (mixed path, tile_n = 0): for each
  * lag-window class (nclen rounded up to 8) the chosen p3 tile width and, where this

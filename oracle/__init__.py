@@ -251,3 +251,45 @@ def run_ref_vcg(randpar, data, nu_chan0, nc, umax, fwhm, flag_key, workdir):
 
 def tmpdir():
     return tempfile.mkdtemp(prefix="amber_oracle_")
+
+
+# ---- cylindrical bispectrum (analysis stage), restated in numpy ----
+
+def blackman_nuttall(m):
+    """Blackman–Nuttall window of length m (mfunc_winds.py:17-31)."""
+    n = np.arange(m)
+    a0, a1, a2, a3 = 0.3635819, 0.4891775, 0.1365995, 0.0106411
+    return a0 - a1 * np.cos(2 * np.pi * n / (m - 1)) + a2 * np.cos(4 * np.pi * n / (m - 1)) - a3 * np.cos(
+        6 * np.pi * n / (m - 1))
+
+
+def cyl_bs(lag, den, nc10, n_cut, mabs_norm, rc, rc_prime, dnu, window=False, div=1.0, float32=False):
+    """Cylindrical bispectrum of one lag array [nclen, nclen]:
+    fold_quadrants (mabs_funcs.py:210-222) of lag/div and of the normaliser ``den``, the ratio
+    over mabs_norm, cut_nan (259-260), optionally the Blackman–Nuttall window of mabs_win
+    (mfunc_winds.py:88-103), then Bdnu2Bk_fft (mabs_funcs.py:325-334) / cylbs_win (122-136).
+
+    ``float32`` repeats the v2 chain's rounding: read_bsout_float_v2 (mabs_funcs.py:190-205)
+    returns float32 arrays, so the reference folds and divides them in float32 before the
+    window (float64) promotes the result.  The v1 chain is float64 from the reader's division
+    by Num onwards."""
+    dt = np.float32 if float32 else np.float64
+
+    def fold(a):
+        a = np.array(a, dtype=dt)
+        lower = a[nc10:, :].copy()
+        lower[1:, :] += a[:nc10, :][::-1, ::-1]
+        return lower
+    lag = np.asarray(lag, dtype=dt)
+    if div != 1.0:
+        lag = lag / np.float64(div)
+    t = fold(lag) / (dt(mabs_norm) if float32 else mabs_norm) / fold(den)
+    d = t[: t.shape[0] - n_cut, n_cut:-n_cut]
+    if window:
+        m = d.shape[1]
+        w2 = np.outer(blackman_nuttall(m), blackman_nuttall(m))
+        d = d * w2[m // 2:, :]
+    n = d.shape[1]
+    res = np.fft.fftshift(np.fft.irfft2(np.fft.ifftshift(d, axes=1), axes=(1, 0), s=(n, n)))
+    length = n * dnu * rc_prime
+    return res * (rc ** 4 * length * length)

@@ -8,7 +8,10 @@ outputs as compressed .npz files:
   est_<name>.npz   — grid sums, counts, ring edges, nc10, channels, and the
                      reference's closed_rings plus, per triangle, its v1
                      (FP64 and float builds) and v2 (FP64) lag arrays;
-  grid_<name>.npz  — visibility records and the reference's GV/sampling sums.
+  grid_<name>.npz  — visibility records and the reference's GV/sampling sums;
+  cylbs_ref.npz    — seeded lag arrays and the cylindrical bispectra that the
+                     reference's analysis Python (mabs_funcs.get_cyl_BS,
+                     mfunc_winds.cylbs_win) computes from them.
 
 Needs the reference sources (make -C oracle ref); run from the repo root:
     python tests/golden/make_golden.py
@@ -89,6 +92,37 @@ def grid_case(name, nc, ngroups, seed, flag_key, fwhm, umax):
     print(name, "NN", nn_ref, "dU", du_ref, "cells hit", int((ntig.sum(axis=2) > 0).sum()))
 
 
+def cylbs_case(nc10=30, seed=11):
+    """The analysis stage's lag→k step, computed by the reference's own Python functions:
+    mabs_funcs.get_cyl_BS (v1 file: counts normalise, the reader divides by Num) and
+    mfunc_winds.cylbs_win (v2 file: mask sums normalise, Blackman–Nuttall window), on seeded lag
+    arrays written in the reference's file formats.  matplotlib is absent here, so a stub stands in
+    for the modules' unused plotting import."""
+    import importlib
+    import types
+    sys.modules.setdefault("matplotlib", types.ModuleType("matplotlib"))
+    sys.modules.setdefault("matplotlib.pyplot", types.ModuleType("matplotlib.pyplot"))
+    sys.path.insert(0, "/root/reference")
+    mf = importlib.import_module("mabs_funcs")
+    nclen = 2 * nc10 + 1
+    mf.nc10, mf.nclen, mf.ncsize = nc10, nclen, nclen * nclen
+    mw = importlib.import_module("mfunc_winds")
+    rng = np.random.default_rng(seed)
+    bl = rng.standard_normal((nclen, nclen)).astype(np.float32)
+    counts = rng.integers(50, 400, (nclen, nclen)).astype(np.int32)
+    mask = rng.uniform(0.5, 2.0, (nclen, nclen)).astype(np.float32)
+    ntri, num = 0.25, 3.5
+    d = oracle.tmpdir()
+    formats.write_bsout_v1(os.path.join(d, formats.bsout_name(1, 3, 2, 1, 1)), ntri, num, bl, counts)
+    formats.write_bsout_v2(os.path.join(d, formats.bsout_name(2, 3, 2, 1, 1)), 1.0 / 64, bl, mask)
+    v1, _ = mf.get_cyl_BS(3, 2, 1, d, 1)
+    v2 = mw.cylbs_win(3, 2, 1, d)
+    np.savez_compressed(os.path.join(OUT, "cylbs_ref.npz"), nc10=nc10, bl=bl, counts=counts, mask=mask, num=num,
+                        n_cut=mf.n_nancut, mabs_norm=mf.mabs_norm, rc=mf.rc, rc_prime=mf.rc_prime, dnu=mf.dnu_mwa,
+                        v1=v1, v2=v2)
+    print("cylbs", v1.shape, v2.shape)
+
+
 if __name__ == "__main__":
     if not oracle.ref_available():
         raise SystemExit("build the reference first: make -C oracle ref")
@@ -96,3 +130,4 @@ if __name__ == "__main__":
         est_case(k, *v)
     for k, v in GRID_CASES.items():
         grid_case(k, *v)
+    cylbs_case()

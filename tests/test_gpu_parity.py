@@ -157,6 +157,41 @@ def test_tile_width_is_numerically_neutral(lib_built):
             np.testing.assert_array_equal(a, b)
 
 
+@pytest.mark.skipif(not oracle.ref_available(), reason="reference build (oracle/_ref) not present")
+def test_config1_full_vs_reference_build(tmp_path, lib_built):
+    """The reference's own CPU-runnable case at full size (128² grid, 32 channels, 8 bins, all 46
+    closed triangles, v1): the reference's sources built with FP64 floats (oracle/_ref/ref_amber64)
+    run on the host cores, and its bsout files are the standard.  Counts and the triangle list are
+    exact, the plain FP64 path is within 1e-10 and the mixed path within 1e-6 of Σ|products| per
+    lag cell."""
+    import amber_b200
+    from amber_b200 import formats
+    real = synth.config1()
+    _, res_path = oracle.run_ref_amber(real, str(tmp_path), version=1, fp64=True)
+    ref_rd = formats.read_closed_rings(res_path)
+    nclen = real.nclen
+    out = {}
+    for prec in ("fp64", "fp64_abs", "mixed"):
+        rdata, res = amber_b200.estimate(real, precision=prec, version=1)
+        out[prec] = (rdata, res)
+    rdata, res64 = out["fp64"]
+    np.testing.assert_array_equal(rdata[:, :3], ref_rd[:, :3])
+    np.testing.assert_allclose(rdata[:, 3], ref_rd[:, 3], rtol=1e-10)
+    assert len(res64) == 46
+    for i, r in enumerate(res64):
+        name = formats.bsout_name(1, r["r1"], r["r2"], r["r3"], 1)
+        ntri, num, bl, nd = formats.read_bsout_v1(f"{res_path}/{name}", nclen, bl_dtype=np.float64)
+        scale = out["fp64_abs"][1][i]["bldnu"].reshape(nclen, nclen) + 1e-300
+        np.testing.assert_array_equal(r["numdnu"].reshape(nclen, nclen), nd)
+        e64 = np.abs(r["bldnu"].reshape(nclen, nclen) - bl) / scale
+        assert e64.max() <= TOL["fp64"], (name, e64.max())
+        em = np.abs(out["mixed"][1][i]["bldnu"].reshape(nclen, nclen) - bl) / scale
+        assert em.max() <= TOL["mixed"], (name, em.max())
+        ng = r["ng1"]
+        np.testing.assert_allclose(num, (ng / real.nn) ** 2 * r["rdata_num"], rtol=1e-12)
+        np.testing.assert_allclose(ntri, num / ng**2, rtol=1e-12)
+
+
 def test_triangle_v1_v2_file_scalars(lib_built):
     import amber_b200
     z = np.load(os.path.join(GOLDEN, "est_flagged48.npz"))
