@@ -38,7 +38,7 @@ EXPORTS = (
     "amber_cuda_triangle_v2", "amber_cuda_triangles", "amber_cuda_triangles_run", "amber_cuda_triangles_fetch",
     "amber_cuda_last_run_stats", "amber_cuda_last_run_breakdown", "amber_cuda_last_run_shape", "amber_cuda_grid_vis",
     "amber_cuda_enqueue", "amber_cuda_wait", "amber_cuda_result", "amber_cuda_engine_stats",
-    "amber_cuda_tile_choices", "amber_cuda_cyl_bs",
+    "amber_cuda_tile_choices", "amber_cuda_cyl_bs", "amber_cuda_grid_vis_collapsed",
 )
 
 
@@ -46,25 +46,6 @@ class AmberError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"libamber_cuda error {code} ({ERRORS.get(code, '?')}): {msg}")
         self.code = code
-
-
-class Request(ctypes.Structure):
-    _fields_ = [("N1", ctypes.c_long), ("nc", ctypes.c_long), ("Du", ctypes.c_double), ("flag_key", ctypes.c_int),
-                ("re_im", ctypes.POINTER(ctypes.c_double)), ("ntig", ctypes.POINTER(ctypes.c_double)),
-                ("Nr", ctypes.c_int), ("ULow", ctypes.POINTER(ctypes.c_double)),
-                ("UHigh", ctypes.POINTER(ctypes.c_double)), ("nc10", ctypes.c_int), ("uf_nc", ctypes.c_int),
-                ("uf_chans", ctypes.POINTER(ctypes.c_int)), ("want_v2", ctypes.c_int)]
-
-
-class EngineInfo(ctypes.Structure):
-    _fields_ = [("requests_done", ctypes.c_long), ("rounds", ctypes.c_long), ("contraction_launches", ctypes.c_long),
-                ("max_active", ctypes.c_long), ("queued", ctypes.c_long), ("active", ctypes.c_long),
-                ("peak_bytes", ctypes.c_size_t), ("budget_bytes", ctypes.c_size_t), ("products", ctypes.c_double),
-                ("busy_ms", ctypes.c_double), ("setup_ms", ctypes.c_double), ("maps_ms", ctypes.c_double),
-                ("contract_ms", ctypes.c_double), ("finish_ms", ctypes.c_double)]
-
-    def as_dict(self):
-        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 class CylBsParams(ctypes.Structure):
@@ -82,6 +63,40 @@ def reference_cylbs_constants():
     nu0, k_b, c = 154.255e6, 1.38e3, 3e8
     rjfac = 2.0 * k_b * nu0 * nu0 / (c * c) / 1e3
     return dict(n_cut=8, mabs_norm=fact * rjfac ** 3, rc=9210.11291939594, rc_prime=17.0, dnu_mhz=0.04)
+
+
+def cylbs_params(window=False, denominator="counts", **const) -> CylBsParams:
+    """amber_cuda_cylbs_params: the reference's analysis constants, overridden by ``const``;
+    ``denominator`` is "counts" (v1 chain) or "mask" (the v2 run's sampling-mask sums)."""
+    if denominator not in ("counts", "mask"):
+        raise ValueError("denominator is 'counts' or 'mask'")
+    k = reference_cylbs_constants()
+    unknown = set(const) - set(k)
+    if unknown:
+        raise TypeError(f"unknown constants {sorted(unknown)}")
+    k.update(const)
+    return CylBsParams(int(k["n_cut"]), int(bool(window)), 0 if denominator == "counts" else 1, float(k["mabs_norm"]),
+                       float(k["rc"]), float(k["rc_prime"]), float(k["dnu_mhz"]))
+
+
+class Request(ctypes.Structure):
+    _fields_ = [("N1", ctypes.c_long), ("nc", ctypes.c_long), ("Du", ctypes.c_double), ("flag_key", ctypes.c_int),
+                ("re_im", ctypes.POINTER(ctypes.c_double)), ("ntig", ctypes.POINTER(ctypes.c_double)),
+                ("Nr", ctypes.c_int), ("ULow", ctypes.POINTER(ctypes.c_double)),
+                ("UHigh", ctypes.POINTER(ctypes.c_double)), ("nc10", ctypes.c_int), ("uf_nc", ctypes.c_int),
+                ("uf_chans", ctypes.POINTER(ctypes.c_int)), ("want_v2", ctypes.c_int),
+                ("cylbs", ctypes.POINTER(CylBsParams))]
+
+
+class EngineInfo(ctypes.Structure):
+    _fields_ = [("requests_done", ctypes.c_long), ("rounds", ctypes.c_long), ("contraction_launches", ctypes.c_long),
+                ("max_active", ctypes.c_long), ("queued", ctypes.c_long), ("active", ctypes.c_long),
+                ("peak_bytes", ctypes.c_size_t), ("budget_bytes", ctypes.c_size_t), ("products", ctypes.c_double),
+                ("busy_ms", ctypes.c_double), ("setup_ms", ctypes.c_double), ("maps_ms", ctypes.c_double),
+                ("contract_ms", ctypes.c_double), ("finish_ms", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 class Opts(ctypes.Structure):
@@ -138,9 +153,12 @@ def load_library():
                                       _fp, _dp, _dp]
     L.amber_cuda_enqueue.argtypes = [_vp, ctypes.POINTER(Request), _i64p]
     L.amber_cuda_wait.argtypes = [_vp, ctypes.c_int64, ctypes.c_int, _ip]
-    L.amber_cuda_result.argtypes = [_vp, ctypes.c_int64, ctypes.c_int, _dp, _dp, _i64p, _dp, _dp]
+    L.amber_cuda_result.argtypes = [_vp, ctypes.c_int64, ctypes.c_int, _dp, _dp, _i64p, _dp, _dp, _dp]
     L.amber_cuda_engine_stats.argtypes = [_vp, ctypes.POINTER(EngineInfo)]
     L.amber_cuda_tile_choices.argtypes = [_vp, ctypes.c_int, _ip, _ip, _fp, _fp]
+    L.amber_cuda_grid_vis_collapsed.argtypes = [_vp, ctypes.c_long, ctypes.c_long, ctypes.c_double, ctypes.c_double,
+                                                ctypes.c_float, ctypes.c_int, ctypes.c_long, ctypes.c_long,
+                                                ctypes.c_long, _fp, _fp, ctypes.c_long, _dp, _dp]
     L.amber_cuda_cyl_bs.argtypes = [_vp, ctypes.POINTER(CylBsParams), _dp, _dp]
     _lib = L
     return L
@@ -293,17 +311,21 @@ class Estimator:
         self._check(self._L.amber_cuda_last_run_stats(self._h, ctypes.byref(p), ctypes.byref(ms)))
         return p.value, ms.value
 
+    def file_num(self, rdata) -> np.ndarray:
+        """The Num a v1 file holds for each calCR row, (Ng1/N1)²·rdata[3] (amber.c:193-202); the v1
+        reader returns bldnu / Num, so it is the tri_div of the get_cyl_BS chain."""
+        rdata = np.asarray(rdata, dtype=np.float64).reshape(-1, 4)
+        g = np.array([self.ng1(int(r1)) / self.n1 for r1 in rdata[:, 0]])
+        return g * g * rdata[:, 3]
+
     def cyl_bs(self, window=False, denominator="counts", tri_div=None, **const):
         """Cylindrical bispectra [ntri, N, N] of the last run (amber_cuda_cyl_bs); ``denominator`` is
         "counts" (v1) or "mask" (the sampling-mask sums of a v2 run); ``tri_div`` divides each
         triangle's sums (Num for the v1 chain); constants default to the reference analysis stage's
         (reference_cylbs_constants)."""
-        k = reference_cylbs_constants()
-        k.update(const)
-        p = CylBsParams(int(k["n_cut"]), int(bool(window)), 0 if denominator == "counts" else 1, float(k["mabs_norm"]),
-                        float(k["rc"]), float(k["rc_prime"]), float(k["dnu_mhz"]))
+        p = cylbs_params(window, denominator, **const)
         ntri, nclen, _ = self.last_run_shape()
-        n = max(nclen - 2 * int(k["n_cut"]), 1)
+        n = max(nclen - 2 * p.n_cut, 1)
         out = np.zeros((max(ntri, 1), n, n))
         td = None
         if tri_div is not None:
@@ -336,21 +358,30 @@ class Estimator:
                                                        None if numtri_ptr is None else ctypes.cast(numtri_ptr, _dp)))
 
     # ---- gridding ---------------------------------------------------------
-    def grid_vis(self, nn, nc, du, umax, nu_chan0, flag_key, randpar, data):
+    def grid_vis(self, nn, nc, du, umax, nu_chan0, flag_key, randpar, data, n_collapse=1):
+        """Grid visibility records (amber_cuda_grid_vis_collapsed): randpar float32 [G, npar],
+        data float32 [G, nchan ≥ nc, nstokes, 3]; the first nc channels are gridded and, with
+        n_collapse > 1, summed in groups of n_collapse.  Returns (complex [NN, H, nc // n_collapse],
+        counts of the same shape)."""
         randpar = np.ascontiguousarray(randpar, dtype=np.float32)
-        data = np.ascontiguousarray(data, dtype=np.float32)
+        data = np.asarray(data, dtype=np.float32)
+        if data.ndim != 4 or data.shape[1] < nc or data.shape[3] != 3 or data.shape[0] != randpar.shape[0]:
+            raise ValueError("data must be [G, nchan >= nc, nstokes, 3] with G = len(randpar)")
+        data = np.ascontiguousarray(data[:, :nc])
         g, npar = randpar.shape
         nstokes = data.shape[2]
         h = nn // 2 + 1
-        ri = np.zeros((nn, h, nc, 2))
-        nt = np.zeros((nn, h, nc))
-        self._check(self._L.amber_cuda_grid_vis(self._h, nn, nc, float(du), float(umax), np.float32(nu_chan0),
-                                                int(flag_key), g, npar, nstokes, _ptr(randpar, _fp), _ptr(data, _fp),
-                                                _ptr(ri, _dp), _ptr(nt, _dp)))
+        ncoll = nc // max(int(n_collapse), 1)
+        ri = np.zeros((nn, h, max(ncoll, 1), 2))
+        nt = np.zeros((nn, h, max(ncoll, 1)))
+        self._check(self._L.amber_cuda_grid_vis_collapsed(self._h, nn, nc, float(du), float(umax),
+                                                          np.float32(nu_chan0), int(flag_key), g, npar, nstokes,
+                                                          _ptr(randpar, _fp), _ptr(data, _fp), int(n_collapse),
+                                                          _ptr(ri, _dp), _ptr(nt, _dp)))
         return ri[..., 0] + 1j * ri[..., 1], nt
 
 
-def _request_of(real, want_v2):
+def _request_of(real, want_v2, cyl=None):
     """Request struct for a synth.Realisation, with the numpy buffers it points to (keep them alive
     until enqueue returns: the library copies them)."""
     ri = np.ascontiguousarray(real.gv, dtype=np.complex128).view(np.float64)
@@ -360,8 +391,8 @@ def _request_of(real, want_v2):
     uf = np.ascontiguousarray(real.uf_chans if real.flag_key == 1 else np.zeros(1), dtype=np.int32)
     q = Request(real.gv.shape[0], real.gv.shape[2], float(real.du), int(real.flag_key), _ptr(ri, _dp), _ptr(nt, _dp),
                 len(lo), _ptr(lo, _dp), _ptr(hi, _dp), int(real.nc10), len(uf) if real.flag_key == 1 else 0,
-                _ptr(uf, _ip), int(bool(want_v2)))
-    return q, (ri, nt, lo, hi, uf)
+                _ptr(uf, _ip), int(bool(want_v2)), None if cyl is None else ctypes.pointer(cyl))
+    return q, (ri, nt, lo, hi, uf, cyl)
 
 
 class Engine:
@@ -372,12 +403,18 @@ class Engine:
     def __init__(self, est: Estimator):
         self.est = est
         self._L = est._L
+        self._cyl_n = {}  # ticket -> N of the cylindrical bispectra it asked for
 
-    def enqueue(self, real, want_v2=True) -> int:
-        q, keep = _request_of(real, want_v2)
+    def enqueue(self, real, want_v2=True, cyl_bs=None) -> int:
+        """Queue a realisation; ``cyl_bs`` (a dict of cylbs_params arguments, e.g.
+        ``dict(window=True, denominator="mask")``) asks for its cylindrical bispectra as well."""
+        cyl = None if cyl_bs is None else cylbs_params(**cyl_bs)
+        q, keep = _request_of(real, want_v2, cyl)
         t = ctypes.c_int64()
         self.est._check(self._L.amber_cuda_enqueue(self.est._h, ctypes.byref(q), ctypes.byref(t)))
         del keep
+        if cyl is not None:
+            self._cyl_n[t.value] = 2 * (int(real.nc10) + 1 - cyl.n_cut) - 1
         return t.value
 
     def wait(self, ticket: int, timeout_ms: int = -1) -> int:
@@ -387,7 +424,8 @@ class Engine:
 
     def result(self, ticket: int, real, want_v2=True):
         """(rdata, bldnu, numdnu, numtri, latency_ms) of a finished request; FP64 lag arrays
-        [ntri, nclen²], int64 counts."""
+        [ntri, nclen²], int64 counts.  A request enqueued with ``cyl_bs`` adds its cylindrical
+        bispectra [ntri, N, N] as a sixth item."""
         n = self.wait(ticket)
         nclen = 2 * real.nc10 + 1
         rd = np.zeros((max(n, 1), 4))
@@ -395,9 +433,13 @@ class Engine:
         nd = np.zeros((max(n, 1), nclen * nclen), dtype=np.int64)
         nt = np.zeros((max(n, 1), nclen * nclen)) if want_v2 else None
         lat = ctypes.c_double()
+        ncyl = self._cyl_n.get(ticket)
+        cy = None if ncyl is None else np.zeros((max(n, 1), ncyl, ncyl))
         self.est._check(self._L.amber_cuda_result(self.est._h, ticket, max(n, 1), _ptr(rd, _dp), _ptr(bl, _dp),
-                                                  _ptr(nd, _i64p), _ptr(nt, _dp), ctypes.byref(lat)))
-        return rd[:n], bl[:n], nd[:n], (None if nt is None else nt[:n]), lat.value
+                                                  _ptr(nd, _i64p), _ptr(nt, _dp), ctypes.byref(lat), _ptr(cy, _dp)))
+        self._cyl_n.pop(ticket, None)
+        out = (rd[:n], bl[:n], nd[:n], (None if nt is None else nt[:n]), lat.value)
+        return out if cy is None else out + (cy[:n],)
 
     def stats(self) -> dict:
         i = EngineInfo()

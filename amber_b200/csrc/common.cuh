@@ -203,6 +203,11 @@ int lag_reduce(amber_cuda_ctx *c, const double *partial, long nunits, long ncsiz
                bool accumulate = false);
 // Device bytes the mixed-precision contraction keeps for the partial tiles of one launch.
 size_t contract_partial_cap(const amber_cuda_ctx *c);
+
+// amber_cuda_cyl_bs: device bytes it may add to a context, and why parameters cannot
+// run on a lag width (nullptr: they can).
+size_t cyl_bs_bytes(int nc10, int n_cut, int ntri);
+const char *cyl_bs_invalid(const amber_cuda_cylbs_params *p, int nc10, int have_mask_sums);
 // Σ_x a·b·c over n points (FP64, deterministic) into out[0].
 int triple_sum(amber_cuda_ctx *c, const double *a, const double *b, const double *cc, long n, double *out);
 

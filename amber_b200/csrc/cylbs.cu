@@ -111,6 +111,30 @@ __global__ void cylbs_cols(const double2 *__restrict__ X, int M, int N, const do
 
 }  // namespace
 
+// Device bytes amber_cuda_cyl_bs may add to a context: its scratch (normalisers, window,
+// one batch of d / X / out) and the twiddle table.
+size_t cyl_bs_bytes(int nc10, int n_cut, int ntri)
+{
+    const long nclen = 2L * nc10 + 1, M = nc10 + 1 - n_cut, N = nclen - 2L * n_cut;
+    if (M < 2 || N < 3) return 0;
+    const size_t per_tri = sizeof(double) * ((size_t)M * N * 3 + (size_t)N * N);
+    const size_t batch = std::max<size_t>(1, std::min<size_t>({(size_t)std::max(ntri, 1), ((size_t)256 << 20) / per_tri,
+                                                               (size_t)65535}));
+    return sizeof(double) * ((size_t)nclen * nclen + N + ntri + 16) + batch * per_tri + 16 * (size_t)N;
+}
+
+// Why the parameters cannot run on a lag width nc10 (nullptr: they can).
+const char *cyl_bs_invalid(const amber_cuda_cylbs_params *p, int nc10, int have_mask_sums)
+{
+    const int nclen = 2 * nc10 + 1, M = nc10 + 1 - p->n_cut, N = nclen - 2 * p->n_cut;
+    if (p->n_cut < 0 || M < 2 || N < 3) return "n_cut leaves no data";
+    if (N > 3072) return "N above 3072";
+    if (!(p->mabs_norm != 0.0)) return "mabs_norm must be non-zero";
+    if (p->denominator != 0 && p->denominator != 1) return "denominator must be 0 (counts) or 1 (mask sums)";
+    if (p->denominator == 1 && !have_mask_sums) return "the mask-sum normaliser needs a v2 run";
+    return nullptr;
+}
+
 }  // namespace amber
 
 using namespace amber;
@@ -125,10 +149,9 @@ extern "C" int amber_cuda_cyl_bs(amber_cuda_ctx *c, const amber_cuda_cylbs_param
     const int nc10 = c->nc10, nclen = 2 * nc10 + 1;
     const int ncut = p->n_cut;
     const int M = nc10 + 1 - ncut, N = nclen - 2 * ncut;
-    if (ncut < 0 || M < 2 || N < 3) return fail(c, AMBER_ERR_ARG, "cyl_bs: n_cut %d leaves no data (nc10=%d)", ncut, nc10);
-    if (!(p->mabs_norm != 0.0)) return fail(c, AMBER_ERR_ARG, "cyl_bs: mabs_norm must be non-zero");
-    // the twiddle table of the transforms sits in shared memory (16·N bytes of the 48 KB default)
-    if (N > 3072) return fail(c, AMBER_ERR_ARG, "cyl_bs: N = %d above 3072", N);
+    // N ≤ 3072: the twiddle table of the transforms sits in shared memory (16·N bytes of the 48 KB default)
+    if (const char *why = cyl_bs_invalid(p, nc10, c->last_v2))
+        return fail(c, AMBER_ERR_ARG, "cyl_bs: %s (n_cut %d, nc10 %d)", why, ncut, nc10);
     cudaSetDevice(c->device);
     const long ncsize = (long)nclen * nclen;
     const int ntri = c->last_ntri;

@@ -58,6 +58,8 @@ struct Request {
     int nc10 = 0;
     std::vector<int> uf;
     int want_v2 = 0;
+    bool want_cyl = false;  // cylindrical bispectra of every triangle as well
+    amber_cuda_cylbs_params cyl{};
     // plan
     std::vector<int> tri;  // closed triangles (host enumeration, as calCR)
     size_t footprint = 0;
@@ -69,7 +71,7 @@ struct Request {
     RunState run;
     bool started = false;
     // results (host)
-    std::vector<double> rdata, bldnu, numtri;
+    std::vector<double> rdata, bldnu, numtri, cyl_out;
     std::vector<int64_t> counts;
     double t_enqueue = 0, t_admit = 0, t_done = 0;
 };
@@ -114,7 +116,8 @@ size_t footprint_of(const Request &r, int precision, long nslots_max)
     // FP64 paths contract in the child context: its partial tiles (anchors × k-splits × lag cells)
     const size_t partial = precision == AMBER_PREC_MIXED ? 0 : sizeof(double) * (size_t)r.nc * 64 * nclen * nclen;
     // the mask maps grow calCR's map buffer; D maps and the builder's intermediate come on top
-    return grid + std::max(staging, partial) + calcr_maps + maps + results + ((size_t)192 << 20);
+    const size_t cyl = r.want_cyl ? cyl_bs_bytes(r.nc10, r.cyl.n_cut, (int)ntri) : 0;
+    return grid + std::max(staging, partial) + calcr_maps + maps + results + cyl + ((size_t)192 << 20);
 }
 
 // Ring slots one batch of the request's largest r1 group would like (all of its rings).
@@ -213,6 +216,24 @@ void Engine::finish(Request *r)
         if (r->want_v2)
             std::copy(res.begin() + (size_t)t * 2 * ncsize + ncsize, res.begin() + (size_t)(t + 1) * 2 * ncsize,
                       r->numtri.begin() + (size_t)t * ncsize);
+    }
+    if (r->want_cyl && ntri > 0) {
+        // the reference's analysis chains: v1 files are read back divided by Num
+        // (amber.c:193-202, mabs_funcs.py:172-187), v2 files as written
+        std::vector<double> num;
+        if (r->cyl.denominator == 0)
+            for (int t = 0; t < ntri; ++t) {
+                const double gfact = (1. * ring_ng1(r->uhigh[r->tri[3 * t]], r->Du)) / (1. * r->N1);
+                num.push_back(gfact * gfact * r->rdata[4 * t + 3]);
+            }
+        s->last_ntri = ntri;
+        s->last_v2 = r->want_v2;
+        const long n = 2 * (r->nc10 + 1 - r->cyl.n_cut) - 1;
+        r->cyl_out.assign((size_t)ntri * n * n, 0.0);
+        if ((rc = amber_cuda_cyl_bs(s, &r->cyl, num.empty() ? nullptr : num.data(), r->cyl_out.data()))) {
+            fail_req(r, rc, s->err);
+            return;
+        }
     }
     r->counts = s->counts;
     info.products += s->last_products;
@@ -378,6 +399,12 @@ int amber_cuda_enqueue(amber_cuda_ctx *c, const amber_cuda_request *q, int64_t *
     r->nc10 = q->nc10;
     if (q->flag_key == 1) r->uf.assign(q->uf_chans, q->uf_chans + q->uf_nc);
     r->want_v2 = q->want_v2 ? 1 : 0;
+    if (q->cylbs) {
+        if (const char *why = amber::cyl_bs_invalid(q->cylbs, q->nc10, r->want_v2))
+            return amber::fail(c, AMBER_ERR_ARG, "enqueue: cylindrical bispectrum parameters: %s", why);
+        r->want_cyl = true;
+        r->cyl = *q->cylbs;
+    }
     r->tri = amber::closed_triangles(r->ulow, r->uhigh);
     const int prec = c->precision;
     r->footprint = amber::footprint_of(*r, prec, amber::slots_wanted(*r));
@@ -417,7 +444,7 @@ int amber_cuda_wait(amber_cuda_ctx *c, int64_t ticket, int timeout_ms, int *ntri
 }
 
 int amber_cuda_result(amber_cuda_ctx *c, int64_t ticket, int max_tri, double *rdata, double *bldnu, int64_t *numdnu,
-                      double *numtri, double *latency_ms)
+                      double *numtri, double *latency_ms, double *cyl_bs)
 {
     if (!c || !c->engine) return AMBER_ERR_ARG;
     Engine *e = c->engine;
@@ -439,6 +466,7 @@ int amber_cuda_result(amber_cuda_ctx *c, int64_t ticket, int max_tri, double *rd
     if (numtri && r->want_v2) std::copy(r->numtri.begin(), r->numtri.end(), numtri);
     if (numdnu)
         for (int t = 0; t < ntri; ++t) std::copy(r->counts.begin(), r->counts.end(), numdnu + (size_t)t * ncsize);
+    if (cyl_bs && r->want_cyl) std::copy(r->cyl_out.begin(), r->cyl_out.end(), cyl_bs);
     if (latency_ms) *latency_ms = r->t_done - r->t_enqueue;
     return AMBER_OK;
 }

@@ -97,20 +97,45 @@ __global__ void sum_kernel(const unsigned *__restrict__ begin, const unsigned *_
     ntig[o] = sn;
 }
 
+// Channel collapse (tgefuncs.c:816-838): output channel col of a cell is the sum of input
+// channels col·n .. col·n + n − 1, added in that order from 0.0 as the reference's loop does.
+__global__ void collapse_kernel(const double *__restrict__ re_im, const double *__restrict__ ntig, long ncell, long nc,
+                                long n, long ncoll, double *__restrict__ re_im_c, double *__restrict__ ntig_c)
+{
+    const long total = ncell * ncoll;
+    for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
+        const long cell = e / ncoll, col = e % ncoll;
+        const long base = cell * nc + col * n;
+        double sr = 0.0, si = 0.0, sn = 0.0;
+        for (long k = 0; k < n; ++k) {
+            sr = __dadd_rn(sr, re_im[2 * (base + k)]);
+            si = __dadd_rn(si, re_im[2 * (base + k) + 1]);
+            sn = __dadd_rn(sn, ntig[base + k]);
+        }
+        re_im_c[2 * e] = sr;
+        re_im_c[2 * e + 1] = si;
+        ntig_c[e] = sn;
+    }
+}
+
 }  // namespace
 
 }  // namespace amber
 
 using namespace amber;
 
-extern "C" int amber_cuda_grid_vis(amber_cuda_ctx *c, long NN, long nc, double dU, double Umax, float nu_chan0,
-                                   int flag_key, long ngroups, long npar, long nstokes, const float *randpar,
-                                   const float *data, double *re_im_out, double *ntig_out)
+extern "C" int amber_cuda_grid_vis_collapsed(amber_cuda_ctx *c, long NN, long nc, double dU, double Umax,
+                                             float nu_chan0, int flag_key, long ngroups, long npar, long nstokes,
+                                             const float *randpar, const float *data, long n_collapse,
+                                             double *re_im_out, double *ntig_out)
 {
     if (!c) return AMBER_ERR_ARG;
     if (NN <= 0 || NN % 2 || nc <= 0 || !(dU > 0) || ngroups < 0 || npar < 2 || nstokes < 1 ||
         (ngroups > 0 && (!randpar || !data)) || !re_im_out || !ntig_out)
         return fail(c, AMBER_ERR_ARG, "bad gridding arguments");
+    if (n_collapse < 1 || nc / n_collapse < 1)
+        return fail(c, AMBER_ERR_ARG, "n_collapse %ld must be in 1..nc (%ld)", n_collapse, nc);
+    const long ncoll = nc / n_collapse;
     if (flag_key != 0 && flag_key != 1) return fail(c, AMBER_ERR_ARG, "flag_key must be 0 or 1");
     const long H = NN / 2 + 1, ncell = NN * H;
     if (ncell >= (long)UINT32_MAX || ngroups >= (long)UINT32_MAX)
@@ -120,11 +145,12 @@ extern "C" int amber_cuda_grid_vis(amber_cuda_ctx *c, long NN, long nc, double d
     const size_t rp_b = sizeof(float) * G * npar, dt_b = sizeof(float) * G * nc * nstokes * 3;
     const size_t kv_b = sizeof(unsigned) * std::max<long>(G, 1);
     const size_t out_b = sizeof(double) * ncell * nc * 3, seg_b = sizeof(unsigned) * ncell * 2;
+    const size_t coll_b = n_collapse > 1 ? sizeof(double) * ncell * ncoll * 3 : 0;
     size_t cub_b = 0;
     cub::DeviceRadixSort::SortPairs(nullptr, cub_b, (unsigned *)nullptr, (unsigned *)nullptr, (unsigned *)nullptr,
                                     (unsigned *)nullptr, (int)std::max<long>(G, 1));
     auto al = [](size_t b) { return (b + 255) / 256 * 256; };
-    size_t total = al(rp_b) + al(dt_b) + 4 * al(kv_b) + al(out_b) + al(seg_b) + al(cub_b) + 256;
+    size_t total = al(rp_b) + al(dt_b) + 4 * al(kv_b) + al(out_b) + al(coll_b) + al(seg_b) + al(cub_b) + 256;
     int rc = ensure(c, c->mixed_scratch, total, "gridding scratch");
     if (rc) return rc;
     char *p = (char *)c->mixed_scratch.p;
@@ -135,6 +161,7 @@ extern "C" int amber_cuda_grid_vis(amber_cuda_ctx *c, long NN, long nc, double d
     unsigned *k1 = (unsigned *)p; p += al(kv_b);
     unsigned *v1 = (unsigned *)p; p += al(kv_b);
     double *d_out = (double *)p; p += al(out_b);
+    double *d_coll = (double *)p; p += al(coll_b);
     unsigned *beg = (unsigned *)p; p += al(seg_b);
     unsigned *end = beg + ncell;
     void *d_cub = p; p += al(cub_b);
@@ -159,18 +186,34 @@ extern "C" int amber_cuda_grid_vis(amber_cuda_ctx *c, long NN, long nc, double d
     dim3 g2((unsigned)ncell, (unsigned)((nc + 127) / 128));
     sum_kernel<<<g2, 128, 0, s>>>(beg, end, v1, d_rp, npar, d_dt, nc, nstokes, flag_key, ncell, d_out,
                                   d_out + 2 * ncell * nc);
+    const double *res = d_out;
+    if (n_collapse > 1) {
+        const long total_c = ncell * ncoll;
+        const unsigned blocks = (unsigned)std::min<long>((total_c + 255) / 256, (long)c->num_sms * 16);
+        collapse_kernel<<<blocks, 256, 0, s>>>(d_out, d_out + 2 * ncell * nc, ncell, nc, n_collapse, ncoll, d_coll,
+                                               d_coll + 2 * ncell * ncoll);
+        res = d_coll;
+    }
     if ((rc = cuda_check(c, cudaGetLastError(), "gridding kernels"))) return rc;
     int bad = 0;
     cudaMemcpyAsync(&bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost, s);
-    if ((rc = cuda_check(c, cudaMemcpyAsync(re_im_out, d_out, sizeof(double) * 2 * ncell * nc,
+    if ((rc = cuda_check(c, cudaMemcpyAsync(re_im_out, res, sizeof(double) * 2 * ncell * ncoll,
                                             cudaMemcpyDeviceToHost, s),
                          "download grid")))
         return rc;
-    if ((rc = cuda_check(c, cudaMemcpyAsync(ntig_out, d_out + 2 * ncell * nc, sizeof(double) * ncell * nc,
+    if ((rc = cuda_check(c, cudaMemcpyAsync(ntig_out, res + 2 * ncell * ncoll, sizeof(double) * ncell * ncoll,
                                             cudaMemcpyDeviceToHost, s),
                          "download counts")))
         return rc;
     if ((rc = cuda_check(c, cudaStreamSynchronize(s), "gridding"))) return rc;
     if (bad) return fail(c, AMBER_ERR_ARG, "a record inside Umax maps outside the %ld x %ld grid", NN, H);
     return AMBER_OK;
+}
+
+extern "C" int amber_cuda_grid_vis(amber_cuda_ctx *c, long NN, long nc, double dU, double Umax, float nu_chan0,
+                                   int flag_key, long ngroups, long npar, long nstokes, const float *randpar,
+                                   const float *data, double *re_im_out, double *ntig_out)
+{
+    return amber_cuda_grid_vis_collapsed(c, NN, nc, dU, Umax, nu_chan0, flag_key, ngroups, npar, nstokes, randpar,
+                                         data, 1, re_im_out, ntig_out);
 }

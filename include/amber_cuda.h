@@ -185,6 +185,19 @@ AMBER_API int amber_cuda_grid_vis(amber_cuda_ctx *ctx, long NN, long nc, double 
                         long ngroups, long npar, long nstokes, const float *randpar, const float *data,
                         double *re_im_out, double *ntig_out);
 
+/* Gridding followed by the channel collapse of the gridding stage
+ * (collapse_channels, 3_vcg/tgefuncs.c:816-838, run with coll_key 1 before
+ * WriteGVnAC_coll / Write_NTiG_coll, 693-724, 752-770): output channel k of a
+ * cell is the sum of the gridded channels k·n_collapse .. k·n_collapse +
+ * n_collapse − 1, added in that order (sums, counts and re/im alike), for
+ * k < nc / n_collapse; trailing channels are dropped.  The outputs hold
+ * NN·(NN/2+1)·(nc/n_collapse) cells' values (·2 for re_im).  n_collapse = 1
+ * is amber_cuda_grid_vis.  The reference's gridding stage collapses by 4. */
+AMBER_API int amber_cuda_grid_vis_collapsed(amber_cuda_ctx *ctx, long NN, long nc, double dU, double Umax,
+                                            float nu_chan0, int flag_key, long ngroups, long npar, long nstokes,
+                                            const float *randpar, const float *data, long n_collapse,
+                                            double *re_im_out, double *ntig_out);
+
 /* ---- batched requests: ensembles of realisations and estimation streams.
  * The reference estimates one realisation per process run (amber.c:21-335);
  * these calls are the batch form of amber_cuda_load_grid_packed +
@@ -206,8 +219,13 @@ AMBER_API int amber_cuda_grid_vis(amber_cuda_ctx *ctx, long NN, long nc, double 
  * and gives its triangle count; a failed request returns its error.
  * amber_cuda_result then copies the outputs into caller buffers and forgets
  * the request: rdata [ntri][4] as amber_cuda_calcr, bldnu and numtri (v2)
- * [ntri][nclen²] FP64, numdnu [ntri][nclen²] int64, and the request's
- * latency in ms from enqueue to completion.  Any output pointer may be NULL. */
+ * [ntri][nclen²] FP64, numdnu [ntri][nclen²] int64, the request's latency in
+ * ms from enqueue to completion and, when the request gave cylbs, the
+ * cylindrical bispectra [ntri][N][N] (N = 2·(nc10 + 1 − n_cut) − 1) as
+ * amber_cuda_cyl_bs makes them from the request's lag arrays, following the
+ * reference's analysis of its files: denominator 0 divides each triangle by its
+ * v1 file's Num (get_cyl_BS), denominator 1 (v2 requests) does not (cylbs_win).
+ * Any output pointer may be NULL. */
 typedef struct amber_cuda_request {
     long N1, nc;
     double Du;
@@ -220,6 +238,7 @@ typedef struct amber_cuda_request {
     int uf_nc;            /* unflagged channel list when flag_key == 1 */
     const int *uf_chans;
     int want_v2;
+    const amber_cuda_cylbs_params *cylbs; /* NULL, or: also the cylindrical bispectra (copied on enqueue) */
 } amber_cuda_request;
 
 typedef struct amber_cuda_engine_info {
@@ -241,7 +260,7 @@ typedef struct amber_cuda_engine_info {
 AMBER_API int amber_cuda_enqueue(amber_cuda_ctx *ctx, const amber_cuda_request *req, int64_t *ticket);
 AMBER_API int amber_cuda_wait(amber_cuda_ctx *ctx, int64_t ticket, int timeout_ms, int *ntri);
 AMBER_API int amber_cuda_result(amber_cuda_ctx *ctx, int64_t ticket, int max_tri, double *rdata, double *bldnu,
-                                int64_t *numdnu, double *numtri, double *latency_ms);
+                                int64_t *numdnu, double *numtri, double *latency_ms, double *cyl_bs);
 AMBER_API int amber_cuda_engine_stats(amber_cuda_ctx *ctx, amber_cuda_engine_info *info);
 
 /* ---- allocation-free FP64 lag contraction of one triangle.  No counterpart

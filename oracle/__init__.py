@@ -228,9 +228,10 @@ def run_ref_amber(real, workdir, version=1, fp64=False, fast=False, rp_begin=0, 
     return json.loads(line[len("AMBER_REF_JSON "):]), res_path
 
 
-def run_ref_vcg(randpar, data, nu_chan0, nc, umax, fwhm, flag_key, workdir):
+def run_ref_vcg(randpar, data, nu_chan0, nc, umax, fwhm, flag_key, workdir, collapse=False):
     """Run the reference's own gridding stage (3_vcg main + tgefuncs) on
-    synthetic records; returns (gv complex [NN,H,nc], ntig, dU, NN)."""
+    synthetic records; returns (gv complex [NN,H,nc], ntig, dU, NN).  ``collapse``
+    runs it with the collapse key set (4 channels per output channel)."""
     from amber_b200 import formats
     vis = os.path.join(workdir, "vis.bin")
     formats.write_vis(vis, randpar, data, nu_chan0, 40.0e3, 1.0)
@@ -239,7 +240,8 @@ def run_ref_vcg(randpar, data, nu_chan0, nc, umax, fwhm, flag_key, workdir):
         f.write(f"{nc}\t{umax!r}\t{fwhm!r}\t1.\n")
     gvp = os.path.join(workdir, "GV_out")
     smp = os.path.join(workdir, "sampling_out")
-    p = subprocess.run([os.path.join(REF_DIR, "ref_vcg"), vis, params, gvp, str(flag_key), "0", "1", smp],
+    p = subprocess.run([os.path.join(REF_DIR, "ref_vcg"), vis, params, gvp, str(flag_key), "1" if collapse else "0", "1",
+                        smp],
                        capture_output=True, text=True, cwd=workdir)
     if p.returncode != 0:
         raise RuntimeError(f"ref_vcg failed: {p.stdout[-1000:]} {p.stderr[-1000:]}")
@@ -251,6 +253,22 @@ def run_ref_vcg(randpar, data, nu_chan0, nc, umax, fwhm, flag_key, workdir):
 
 def tmpdir():
     return tempfile.mkdtemp(prefix="amber_oracle_")
+
+
+def collapse_channels(gv, ntig, n):
+    """collapse_channels (3_vcg/tgefuncs.c:816-838): output channel k of every cell is the sum
+    of channels k·n .. k·n + n − 1, added in that order from 0.0; trailing channels dropped.
+    gv complex [NN, H, nc], ntig [NN, H, nc]."""
+    ncoll = gv.shape[2] // n
+    re = np.zeros(gv.shape[:2] + (ncoll,))
+    im = np.zeros_like(re)
+    nt = np.zeros_like(re)
+    for k in range(n):
+        sl = slice(k, ncoll * n, n)
+        re = re + gv.real[:, :, sl]
+        im = im + gv.imag[:, :, sl]
+        nt = nt + ntig[:, :, sl]
+    return re + 1j * im, nt
 
 
 # ---- cylindrical bispectrum (analysis stage), restated in numpy ----
@@ -283,7 +301,9 @@ def cyl_bs(lag, den, nc10, n_cut, mabs_norm, rc, rc_prime, dnu, window=False, di
     lag = np.asarray(lag, dtype=dt)
     if div != 1.0:
         lag = lag / np.float64(div)
-    t = fold(lag) / (dt(mabs_norm) if float32 else mabs_norm) / fold(den)
+    # like the reference, divide the whole folded array; empty edge cells (0/0) fall in the cut
+    with np.errstate(divide="ignore", invalid="ignore"):
+        t = fold(lag) / (dt(mabs_norm) if float32 else mabs_norm) / fold(den)
     d = t[: t.shape[0] - n_cut, n_cut:-n_cut]
     if window:
         m = d.shape[1]

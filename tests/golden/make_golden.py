@@ -8,7 +8,8 @@ outputs as compressed .npz files:
   est_<name>.npz   — grid sums, counts, ring edges, nc10, channels, and the
                      reference's closed_rings plus, per triangle, its v1
                      (FP64 and float builds) and v2 (FP64) lag arrays;
-  grid_<name>.npz  — visibility records and the reference's GV/sampling sums;
+  grid_<name>.npz  — visibility records and the reference's GV/sampling sums
+                     (coll_*: with the collapse key set);
   cylbs_ref.npz    — seeded lag arrays and the cylindrical bispectra that the
                      reference's analysis Python (mabs_funcs.get_cyl_BS,
                      mfunc_winds.cylbs_win) computes from them.
@@ -76,9 +77,13 @@ GRID_CASES = {
     "flag1": (5, 2000, 11, 1, 1480.73, 30.0),
     "flag0": (4, 1200, 12, 0, 1480.73, 25.0),
 }
+# the same, run with the collapse key (4 channels per output channel; 9 → 2, one dropped)
+GRID_COLL_CASES = {
+    "coll_flag1": (9, 600, 13, 1, 1480.73, 25.0),
+}
 
 
-def grid_case(name, nc, ngroups, seed, flag_key, fwhm, umax):
+def grid_case(name, nc, ngroups, seed, flag_key, fwhm, umax, collapse=False):
     # dU the reference derives from the beam (tgefuncs.c:306-309)
     import math
     theta0 = 0.6 * fwhm * math.pi / (180. * 60.)
@@ -86,9 +91,10 @@ def grid_case(name, nc, ngroups, seed, flag_key, fwhm, umax):
     nn = 2 * int(math.ceil(umax / du))
     randpar, data = synth.make_visibilities(nn, du, nc, ngroups, seed, umax=umax * 1.02)
     gv, ntig, du_ref, nn_ref = oracle.run_ref_vcg(randpar, data, np.float32(synth.NU0), nc, umax, fwhm, flag_key,
-                                                  oracle.tmpdir())
+                                                  oracle.tmpdir(), collapse=collapse)
     np.savez_compressed(os.path.join(OUT, f"grid_{name}.npz"), randpar=randpar, data=data, nu0=np.float32(synth.NU0),
-                        du=du_ref, nn=nn_ref, umax=umax, flag_key=flag_key, gv=gv, ntig=ntig)
+                        du=du_ref, nn=nn_ref, umax=umax, flag_key=flag_key, gv=gv, ntig=ntig, fwhm=fwhm,
+                        n_collapse=4 if collapse else 1)
     print(name, "NN", nn_ref, "dU", du_ref, "cells hit", int((ntig.sum(axis=2) > 0).sum()))
 
 
@@ -130,4 +136,6 @@ if __name__ == "__main__":
         est_case(k, *v)
     for k, v in GRID_CASES.items():
         grid_case(k, *v)
+    for k, v in GRID_COLL_CASES.items():
+        grid_case(k, *v, collapse=True)
     cylbs_case()

@@ -68,3 +68,48 @@ def test_driver_v2_files(tmp_path):
         inv, bl, nt = formats.read_bsout_v2(f, n)
         assert inv == z["inv_ng"][i]
         assert np.abs(nt - z["numtri_v2"][i]).max() <= 1e-6 * np.abs(z["numtri_v2"][i]).max()
+
+
+def _run_vcg(tmp, z, collapse, fwhm=1480.73):
+    from amber_b200 import build
+    build.build()
+    vis = tmp / "vis.bin"
+    formats.write_vis(vis, z["randpar"], z["data"], np.float32(z["nu0"]), 40.0e3, 1.0)
+    params = tmp / "inputparameters"
+    params.write_text(f"{z['data'].shape[1]}\t{float(z['umax'])!r}\t{fwhm!r}\t1.\n")
+    gv, smp = tmp / "GV_gpu", tmp / "sampling_gpu"
+    exe = build.VCG_DRIVER
+    p = subprocess.run([exe, str(vis), str(params), str(gv), str(int(z["flag_key"])), str(int(collapse)), "1",
+                        str(smp)], capture_output=True, text=True, cwd=tmp)
+    assert p.returncode == 0, p.stderr
+    stats = json.loads([ln for ln in p.stdout.splitlines() if ln.startswith("VCG_GPU_JSON ")][-1][13:])
+    return gv, smp, stats
+
+
+@pytest.mark.parametrize("case,collapse", [("grid_coll_flag1", True), ("grid_flag0", False)])
+def test_vcg_driver_matches_reference_files(tmp_path, case, collapse):
+    """vcg_gpu (the gridding stage's executable): same arguments, same GV and sampling files as the
+    reference's 3_vcg run on the same records (bit-identical values; byte-identical files when the
+    reference build is present)."""
+    import oracle
+    z = np.load(os.path.join(GOLDEN, case + ".npz"))
+    fwhm = float(z["fwhm"]) if "fwhm" in z.files else 1480.73
+    gv_path, smp_path, stats = _run_vcg(tmp_path, z, collapse, fwhm)
+    nc_out = z["gv"].shape[2]
+    assert stats["NN"] == int(z["nn"]) and stats["nc_out"] == nc_out and stats["dU"] == float(z["du"])
+    assert os.path.getsize(gv_path) == 28 + z["gv"].size * 16
+    gv, du, fk = formats.read_gv(gv_path)
+    assert du == float(z["du"]) and fk == int(z["flag_key"])
+    assert np.array_equal(gv.real, z["gv"].real) and np.array_equal(gv.imag, z["gv"].imag)
+    assert np.array_equal(formats.read_sampling(smp_path, int(z["nn"]), nc_out), z["ntig"])
+    if oracle.ref_available():
+        ref = tmp_path / "ref"
+        ref.mkdir()
+        vis = tmp_path / "vis.bin"
+        params = tmp_path / "inputparameters"
+        p = subprocess.run([os.path.join(oracle.REF_DIR, "ref_vcg"), str(vis), str(params), str(ref / "GV"),
+                            str(int(z["flag_key"])), str(int(collapse)), "1", str(ref / "sampling")],
+                           capture_output=True, text=True, cwd=ref)
+        assert p.returncode == 0, p.stdout[-500:]
+        assert (ref / "GV").read_bytes() == gv_path.read_bytes()
+        assert (ref / "sampling").read_bytes() == smp_path.read_bytes()

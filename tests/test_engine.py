@@ -124,3 +124,56 @@ def test_bad_request_and_timeout(lib_built):
         eng.result(t, big)
         with pytest.raises(amber_b200.AmberError):
             eng.wait(t)  # the result has been collected: unknown ticket
+
+
+def _cyl_reals():
+    # nc10 = 19, 35, 11 with the default cut of 8: every folded, cut lag cell has triplets
+    e = _ensemble()
+    return [e[1], e[4], synth.tiny(48, 24, seed=46, nbins=5, hi=21.0, nc10=11)]
+
+
+def test_engine_returns_cylindrical_bispectra(lib_built):
+    """Requests that ask for cylindrical bispectra get what the single-realisation path's
+    amber_cuda_cyl_bs gives (v1: divided by the file Num, v2: mask sums and window), and those
+    match the oracle's restatement of the reference's analysis on the same lag arrays."""
+    import amber_b200
+    reals = _cyl_reals()
+    k = amber_b200.reference_cylbs_constants()
+    with amber_b200.Estimator(precision="mixed") as est:
+        eng = amber_b200.Engine(est)
+        t1 = [eng.enqueue(r, want_v2=False, cyl_bs={}) for r in reals]
+        t2 = [eng.enqueue(r, want_v2=True, cyl_bs=dict(window=True, denominator="mask")) for r in reals]
+        o1 = [eng.result(t, r, want_v2=False) for t, r in zip(t1, reals)]
+        o2 = [eng.result(t, r, want_v2=True) for t, r in zip(t2, reals)]
+    with amber_b200.Estimator(precision="mixed") as est:
+        for r, a, b in zip(reals, o1, o2):
+            const = dict(nc10=r.nc10, n_cut=k["n_cut"], mabs_norm=k["mabs_norm"], rc=k["rc"], rc_prime=k["rc_prime"],
+                         dnu=k["dnu_mhz"])
+            nclen = 2 * r.nc10 + 1
+            rdata, _ = amber_b200.estimate(r, version=1, est=est)
+            num = est.file_num(rdata)
+            single = est.cyl_bs(tri_div=num)
+            assert a[5].shape == single.shape
+            assert np.abs(a[5] - single).max() <= 1e-12 * np.abs(single).max()
+            for i in range(len(rdata)):
+                want = oracle.cyl_bs(a[1][i].reshape(nclen, nclen), a[2][i].reshape(nclen, nclen), div=num[i], **const)
+                assert np.abs(a[5][i] - want).max() <= 1e-10 * np.abs(want).max()
+            amber_b200.estimate(r, version=2, est=est)
+            single = est.cyl_bs(window=True, denominator="mask")
+            assert np.abs(b[5] - single).max() <= 1e-12 * np.abs(single).max()
+            for i in range(len(rdata)):
+                want = oracle.cyl_bs(b[1][i].reshape(nclen, nclen), b[3][i].reshape(nclen, nclen), window=True,
+                                     **const)
+                assert np.abs(b[5][i] - want).max() <= 1e-10 * np.abs(want).max()
+
+
+def test_engine_rejects_bad_cylindrical_parameters(lib_built):
+    import amber_b200
+    r = _cyl_reals()[2]
+    with amber_b200.Estimator(precision="mixed") as est:
+        eng = amber_b200.Engine(est)
+        for kw, v2 in ((dict(n_cut=12), True), (dict(denominator="mask"), False), (dict(mabs_norm=0.0), True)):
+            with pytest.raises(amber_b200.AmberError) as e:
+                eng.enqueue(r, want_v2=v2, cyl_bs=kw)
+            assert e.value.code == -1
+        assert eng.stats()["queued"] == 0
