@@ -38,7 +38,7 @@ EXPORTS = (
     "amber_cuda_triangle_v2", "amber_cuda_triangles", "amber_cuda_triangles_run", "amber_cuda_triangles_fetch",
     "amber_cuda_last_run_stats", "amber_cuda_last_run_breakdown", "amber_cuda_last_run_shape", "amber_cuda_grid_vis",
     "amber_cuda_enqueue", "amber_cuda_wait", "amber_cuda_result", "amber_cuda_engine_stats",
-    "amber_cuda_tile_choices", "amber_cuda_cyl_bs", "amber_cuda_grid_vis_collapsed",
+    "amber_cuda_tile_choices", "amber_cuda_cyl_bs", "amber_cuda_grid_vis_collapsed", "amber_cuda_cl_dnu",
 )
 
 
@@ -159,6 +159,7 @@ def load_library():
     L.amber_cuda_grid_vis_collapsed.argtypes = [_vp, ctypes.c_long, ctypes.c_long, ctypes.c_double, ctypes.c_double,
                                                 ctypes.c_float, ctypes.c_int, ctypes.c_long, ctypes.c_long,
                                                 ctypes.c_long, _fp, _fp, ctypes.c_long, _dp, _dp]
+    L.amber_cuda_cl_dnu.argtypes = [_vp, ctypes.c_int, ctypes.c_double, ctypes.c_double, _dp, _dp, _dp, _ip]
     L.amber_cuda_cyl_bs.argtypes = [_vp, ctypes.POINTER(CylBsParams), _dp, _dp]
     _lib = L
     return L
@@ -310,6 +311,17 @@ class Estimator:
         p, ms = ctypes.c_double(), ctypes.c_double()
         self._check(self._L.amber_cuda_last_run_stats(self._h, ctypes.byref(p), ctypes.byref(ms)))
         return p.value, ms.value
+
+    def cl_dnu(self, nb=15, umin=1.0, umax=500.0) -> dict:
+        """MAPS two-point function of the loaded grid (amber_cuda_cl_dnu; maps.c's NB = 15, Umin1 = 1,
+        Umax1 = 500 by default): dict(cldnu [nb, nc], numdnu [nc], binu [nb], num [nb])."""
+        if self.nc is None:
+            raise AmberError(-6, "cl_dnu: no grid loaded")
+        out = dict(cldnu=np.zeros((nb, self.nc)), numdnu=np.zeros(self.nc), binu=np.zeros(nb),
+                   num=np.zeros(nb, dtype=np.int32))
+        self._check(self._L.amber_cuda_cl_dnu(self._h, int(nb), float(umin), float(umax), _ptr(out["cldnu"], _dp),
+                                              _ptr(out["numdnu"], _dp), _ptr(out["binu"], _dp), _ptr(out["num"], _ip)))
+        return out
 
     def file_num(self, rdata) -> np.ndarray:
         """The Num a v1 file holds for each calCR row, (Ng1/N1)²·rdata[3] (amber.c:193-202); the v1

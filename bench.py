@@ -292,6 +292,39 @@ def config4_section(amber_b200, synth, dev, args):
             "generation_s": t_gen}
 
 
+def maps_section(amber_b200, synth, dev):
+    """The MAPS two-point function (amber_cuda_cl_dnu; maps.c's 15 bins from 1 to 500) of the
+    single-realisation grid, against the reference's own cl_dnu pair loop (oracle/_ref/ref_maps,
+    one host thread as maps.c runs it) on the same grid."""
+    real = synth.config2(seed=1)
+    with amber_b200.Estimator(device=dev, precision="fp64") as est:
+        est.load_grid(real.gv, real.counts, real.du, real.flag_key)
+        out = est.cl_dnu()  # warm-up
+        times = []
+        for _ in range(5):
+            t0 = time.perf_counter()
+            out = est.cl_dnu()
+            times.append(time.perf_counter() - t0)
+    nc = real.gv.shape[2]
+    res = {"workload": "MAPS C_l(dnu) of the single-realisation grid: 256^2 cells, 128 channels, 15 log bins 1-500",
+           "pairs": nc * (nc + 1) // 2, "call_ms_median": 1e3 * float(np.median(times)),
+           "call_ms_min": 1e3 * float(min(times))}
+    try:
+        import oracle
+        if oracle.ref_available():
+            wd = tempfile.mkdtemp(prefix="amber_maps_")
+            try:
+                ref, _ = oracle.run_ref_maps(real, wd)
+            finally:
+                shutil.rmtree(wd, ignore_errors=True)
+            res["reference_pairs_s"] = ref["pairs_s"]
+            res["speedup_vs_reference"] = ref["pairs_s"] / (res["call_ms_median"] * 1e-3)
+            res["bit_identical"] = all(np.array_equal(out[k], ref[k]) for k in ("cldnu", "numdnu", "binu", "num"))
+    except Exception as e:  # the comparison is a report, not the measurement
+        res["reference_error"] = str(e)[:200]
+    return res
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -303,6 +336,8 @@ def main():
     ap.add_argument("--tri-subset", default="", help="comma-separated triangle indices (profiling runs only)")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble measurement")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving-stream measurement")
+    ap.add_argument("--maps", action="store_true",
+                    help="measure the MAPS two-point function (amber_cuda_cl_dnu) instead of the default step")
     ap.add_argument("--config4", action="store_true",
                     help="measure a fixed sample of the large cube (512^2, 384 channels) instead of the default step")
     args = ap.parse_args()
@@ -329,6 +364,13 @@ def main():
             print(json.dumps(dict(metric=METRIC, impl="amber_b200", n_gpus=1, higher_is_better=True,
                                   dtype="int8 tensor-core digits, int32 accumulate, fp64 reduce", data="synthetic",
                                   config={"workload": c4["workload"]}, **{k: v for k, v in c4.items() if k != "workload"})))
+        return 0
+
+    if args.maps:
+        if rank == 0:
+            m = maps_section(amber_b200, synth, local)
+            print(json.dumps(dict(impl="amber_b200", n_gpus=1, dtype="f64", data="synthetic",
+                                  config={"workload": m["workload"]}, **{k: v for k, v in m.items() if k != "workload"})))
         return 0
 
     real = synth.config2(seed=1 + rank)

@@ -139,6 +139,19 @@ AMBER_API int amber_cuda_last_run_shape(const amber_cuda_ctx *ctx, int *ntri, in
 AMBER_API int amber_cuda_last_run_breakdown(const amber_cuda_ctx *ctx, double *ms_maps, double *ms_contract,
                                             double *ms_reduce, long *kernel_launches, long *contract_launches);
 
+/* ---- MAPS two-point function: replaces 4_fbe/maps.c:179-210, which calls
+ * cl_dnu (4_fbe/amber_funcs.c:1418-1488) for every channel pair nn1 <= nn2 of
+ * the normalised grid.  On the grid the context holds (amber_cuda_load_grid*),
+ * per log bin b of U = |(ia, j)|·Du in [umin, umax) (NB bins; maps.c uses 15,
+ * 1 and 500): cldnu [NB][nc] = Σ over pairs with nn2 − nn1 = Δ of the pair's
+ * binned mean of (Re1·Re2 + Im1·Im2)·NTiG1; numdnu [nc] = the pair count per
+ * Δ; binu [NB] and num [NB] = the mean U and the sample count of the last pair
+ * (nn1 = nn2 = nc − 1), which is what maps.c writes beside every row.  The
+ * sums follow the reference's order and roundings, so the values are
+ * bit-identical to the reference's.  numdnu, binu and num may be NULL. */
+AMBER_API int amber_cuda_cl_dnu(amber_cuda_ctx *ctx, int NB, double umin, double umax, double *cldnu,
+                                double *numdnu, double *binu, int *num);
+
 /* ---- cylindrical bispectrum: the analysis stage's lag→k step on the device.
  * Replaces mabs_funcs.py get_cyl_BS (376-389: fold_quadrants 210-222, cut_nan
  * 259-260, Bdnu2Bk_fft 325-334) and, with window = 1, mfunc_winds.py

@@ -43,6 +43,9 @@ def lib():
         L.orc_grid_vis.argtypes = [ctypes.c_long, ctypes.c_long, ctypes.c_double, ctypes.c_double, ctypes.c_float,
                                    ctypes.c_int, ctypes.c_long, ctypes.c_long, ctypes.c_long, _fp, _fp, _dp, _dp]
         L.orc_normalize.argtypes = [ctypes.c_long, ctypes.c_long, _dp, _dp]
+        L.orc_cl_dnu.restype = None
+        L.orc_cl_dnu.argtypes = [ctypes.c_long, ctypes.c_long, ctypes.c_double, _dp, _dp, ctypes.c_int, ctypes.c_double,
+                                 ctypes.c_double, _dp, _dp, _dp, _dp, _ip]
         L.orc_uavg.argtypes = [ctypes.c_int, _dp, _dp, _dp]
         L.orc_triangles.restype = ctypes.c_int
         L.orc_triangles.argtypes = [ctypes.c_int, _dp, _ip, ctypes.c_int]
@@ -201,7 +204,7 @@ def estimate(real, version=1, tri_subset=None, with_absscale=False):
 # ---- the reference's own code, built from its sources (oracle/_ref) -------------------------
 
 def ref_available():
-    return all(os.path.exists(os.path.join(REF_DIR, b)) for b in ("ref_amber", "ref_amber64", "ref_vcg"))
+    return all(os.path.exists(os.path.join(REF_DIR, b)) for b in ("ref_amber", "ref_amber64", "ref_vcg", "ref_maps"))
 
 
 def run_ref_amber(real, workdir, version=1, fp64=False, fast=False, rp_begin=0, rp_end=-1, nthreads=None,
@@ -253,6 +256,45 @@ def run_ref_vcg(randpar, data, nu_chan0, nc, umax, fwhm, flag_key, workdir, coll
 
 def tmpdir():
     return tempfile.mkdtemp(prefix="amber_oracle_")
+
+
+def cl_dnu(real, nb=15, umin=1.0, umax=500.0):
+    """MAPS two-point function (orc_cl_dnu: amber_funcs.c:1418-1488 driven as 4_fbe/maps.c:179-210)
+    of a synth.Realisation's normalised grid.  Returns dict(cldnu [nb, nc], cldnu_abs, numdnu [nc],
+    binu [nb], num [nb]) — binu/num as the last channel pair leaves them."""
+    gvn, ntn = normalize(real.gv, real.counts)
+    nn, h, nc = ntn.shape
+    re_im = np.ascontiguousarray(np.stack([gvn.real, gvn.imag], axis=-1))
+    ntn = np.ascontiguousarray(ntn)
+    out = dict(cldnu=np.zeros((nb, nc)), cldnu_abs=np.zeros((nb, nc)), numdnu=np.zeros(nc), binu=np.zeros(nb),
+               num=np.zeros(nb, dtype=np.int32))
+    lib().orc_cl_dnu(nn, nc, float(real.du), _p(re_im, _dp), _p(ntn, _dp), nb, float(umin), float(umax),
+                     _p(out["cldnu"], _dp), _p(out["cldnu_abs"], _dp), _p(out["numdnu"], _dp), _p(out["binu"], _dp),
+                     _p(out["num"], _ip))
+    return out
+
+
+def run_ref_maps(real, workdir, nb=15, umin=1.0, umax=500.0, rlzn=1):
+    """The reference's own cl_dnu over every channel pair (oracle/_ref/ref_maps).  Returns
+    (dict(cldnu, numdnu, binu, num at full precision; pairs_s: the pair loop's time), path of the
+    maps.c-style text file)."""
+    from amber_b200 import formats
+    data_path = os.path.join(workdir, "data")
+    real.write(data_path, rlzn)
+    params = os.path.join(workdir, "input_params_ess")
+    formats.write_input_params_ess(params, 154.255e6, 40.0e3, 1.0, data_path)
+    txt, binf = os.path.join(workdir, "cldnu"), os.path.join(workdir, "cldnu.bin")
+    p = subprocess.run([os.path.join(REF_DIR, "ref_maps"), str(rlzn), params, str(nb), repr(float(umin)),
+                        repr(float(umax)), txt, binf], capture_output=True, text=True, cwd=workdir)
+    if p.returncode != 0:
+        raise RuntimeError(f"ref_maps failed: {p.stdout[-1000:]} {p.stderr[-1000:]}")
+    nc = real.gv.shape[2]
+    timing = json.loads([ln for ln in p.stdout.splitlines() if ln.startswith("MAPS_REF_JSON ")][-1][14:])
+    raw = open(binf, "rb").read()
+    d = np.frombuffer(raw, dtype=np.float64, count=nb * nc + nc + nb)
+    num = np.frombuffer(raw, dtype=np.int32, offset=8 * (nb * nc + nc + nb), count=nb)
+    return dict(cldnu=d[: nb * nc].reshape(nb, nc).copy(), numdnu=d[nb * nc: nb * nc + nc].copy(),
+                binu=d[nb * nc + nc:].copy(), num=num.copy(), pairs_s=timing["pairs_s"]), txt
 
 
 def collapse_channels(gv, ntig, n):

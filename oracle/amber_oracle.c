@@ -293,3 +293,71 @@ ORC_EXPORT void orc_triangle_absscale(long K, long nc, int nc10, int uf_nc, cons
     }
     free(pb);
 }
+
+/* ---- f3: MAPS two-point function, amber_funcs.c:1418-1488 (cl_dnu) driven as
+ * 4_fbe/maps.c:179-210 does: for every channel pair nn1 <= nn2, per log bin of
+ * U = |(ia, j)|·Du in [umin, umax):
+ *   no    = Σ NTiG[nn1],  pksum = Σ (Re1·Re2 + Im1·Im2)·NTiG[nn1],  usum = Σ U·NTiG[nn1]
+ * (cells in index order), binps = pksum/no, binu = usum/no where no != 0; then
+ * cldnu[b][nn2−nn1] += binps (nn1 ascending) and numdnu[nn2−nn1] += 1.  binu and
+ * num are what the last pair (nn1 = nn2 = nc−1) leaves, as maps.c prints them.
+ * The grid is the normalised one (normalize_data).  A cell whose bin index
+ * rounds to NB (U just below umax) is skipped; the reference would write past
+ * its arrays there.  cldnu_abs (may be NULL) is the same sum over |terms|. */
+ORC_EXPORT void orc_cl_dnu(long N1, long nc, double Du, const double *re_im, const double *ntig, int NB, double umin,
+                           double umax, double *cldnu, double *cldnu_abs, double *numdnu, double *binu, int *num)
+{
+    const long H = N1 / 2 + 1;
+    double *usum = (double *)calloc(NB, sizeof(double));
+    double *pksum = (double *)calloc(NB, sizeof(double));
+    double *pkabs = (double *)calloc(NB, sizeof(double));
+    int *no = (int *)calloc(NB, sizeof(int));
+    const double binsiz = log10(umax / umin) / (1. * NB);
+    memset(cldnu, 0, sizeof(double) * NB * nc);
+    if (cldnu_abs) memset(cldnu_abs, 0, sizeof(double) * NB * nc);
+    memset(numdnu, 0, sizeof(double) * nc);
+    for (long n1 = 0; n1 < nc; ++n1)
+        for (long n2 = n1; n2 < nc; ++n2) {
+            for (int i = 0; i < NB; ++i) {
+                no[i] = 0;
+                usum[i] = pksum[i] = pkabs[i] = 0.0;
+            }
+            for (long i = 0; i < N1; ++i)
+                for (long j = 0; j < H; ++j) {
+                    const long index = i * H + j;
+                    const long ia = (i > N1 / 2) ? (N1 - i) : i;
+                    const double uu = sqrt(1. * (ia * ia + j * j)) * Du;
+                    if (uu >= umin && uu < umax) {
+                        const double *a = re_im + 2 * (index * nc + n1), *b = re_im + 2 * (index * nc + n2);
+                        double numer = a[0] * b[0] + a[1] * b[1];
+                        const double w = ntig[index * nc + n1];
+                        numer *= w;
+                        const int tmp = (int)floor(log10(uu / umin) / binsiz);
+                        if (tmp < 0 || tmp >= NB) continue;
+                        no[tmp] += w;
+                        pksum[tmp] += numer;
+                        pkabs[tmp] += fabs(numer);
+                        usum[tmp] += uu * w;
+                    }
+                }
+            for (int i = 0; i < NB; ++i)
+                if (no[i] != 0) {
+                    usum[i] /= (1. * no[i]);
+                    pksum[i] /= (1. * no[i]);
+                    pkabs[i] /= (1. * no[i]);
+                }
+            numdnu[n2 - n1] += 1.;
+            for (int i = 0; i < NB; ++i) {
+                cldnu[i * nc + (n2 - n1)] += pksum[i];
+                if (cldnu_abs) cldnu_abs[i * nc + (n2 - n1)] += pkabs[i];
+            }
+        }
+    for (int i = 0; i < NB; ++i) {
+        binu[i] = usum[i];
+        num[i] = no[i];
+    }
+    free(usum);
+    free(pksum);
+    free(pkabs);
+    free(no);
+}

@@ -10,6 +10,8 @@ outputs as compressed .npz files:
                      (FP64 and float builds) and v2 (FP64) lag arrays;
   grid_<name>.npz  — visibility records and the reference's GV/sampling sums
                      (coll_*: with the collapse key set);
+  maps_<name>.npz  — a grid and the MAPS two-point function the reference's own
+                     cl_dnu computes from it (oracle/_ref/ref_maps);
   cylbs_ref.npz    — seeded lag arrays and the cylindrical bispectra that the
                      reference's analysis Python (mabs_funcs.get_cyl_BS,
                      mfunc_winds.cylbs_win) computes from them.
@@ -129,6 +131,20 @@ def cylbs_case(nc10=30, seed=11):
     print("cylbs", v1.shape, v2.shape)
 
 
+def maps_case(name="maps_flagged40", seed=51):
+    """The reference's own cl_dnu over every channel pair (ref_maps: amber_funcs.c unchanged, driven
+    as 4_fbe/maps.c drives it) on a small flagged realisation, with maps.c's bins (15, 1, 500) and a
+    finer set (24 bins from 0.7 to 30)."""
+    real = synth.tiny(40, 10, seed=seed, nbins=4, hi=18.0, flagged=[3, 8])
+    out = dict(gv=real.gv, counts=real.counts, du=real.du)
+    for tag, (nb, umin, umax) in {"maps": (15, 1.0, 500.0), "fine": (24, 0.7, 30.0)}.items():
+        r, _ = oracle.run_ref_maps(real, oracle.tmpdir(), nb, umin, umax)
+        out.update({f"{tag}_{k}": v for k, v in r.items()})
+        out[f"{tag}_bins"] = np.array([nb, umin, umax])
+    np.savez_compressed(os.path.join(OUT, f"{name}.npz"), **out)
+    print(name, "nonempty bins", int((out["maps_num"] > 0).sum()), int((out["fine_num"] > 0).sum()))
+
+
 if __name__ == "__main__":
     if not oracle.ref_available():
         raise SystemExit("build the reference first: make -C oracle ref")
@@ -139,3 +155,4 @@ if __name__ == "__main__":
     for k, v in GRID_COLL_CASES.items():
         grid_case(k, *v, collapse=True)
     cylbs_case()
+    maps_case()
