@@ -1,8 +1,8 @@
 """Build libamber_cuda.so in-tree for sm_100a (nvcc, no JIT cache).
 
 ``python -m amber_b200.build`` or ``amber_b200.build.build()``; also builds
-the C drivers ``amber_gpu`` (estimator stage) and ``vcg_gpu`` (gridding stage)
-next to the library.
+the C drivers ``amber_gpu`` (estimator stage), ``vcg_gpu`` (gridding stage)
+and ``maps_gpu`` (the MAPS two-point function) next to the library.
 """
 from __future__ import annotations
 
@@ -17,6 +17,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libamber_cuda.so")
 DRIVER = os.path.join(HERE, "amber_gpu")
 VCG_DRIVER = os.path.join(HERE, "vcg_gpu")
+MAPS_DRIVER = os.path.join(HERE, "maps_gpu")
 SOURCES = ["api.cu", "maps.cu", "contract64.cu", "contract_tc.cu", "contract_i8.cu", "grid.cu", "noalloc.cu", "engine.cu", "cylbs.cu", "cldnu.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -53,7 +54,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
             objs.append(o)
         cmd = [nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-lcuda"]
         subprocess.run(cmd, check=True)
-    for exe, name in ((DRIVER, "amber_gpu.c"), (VCG_DRIVER, "vcg_gpu.c")):
+    for exe, name in ((DRIVER, "amber_gpu.c"), (VCG_DRIVER, "vcg_gpu.c"), (MAPS_DRIVER, "maps_gpu.c")):
         drv_src = os.path.join(HERE, "driver", name)
         if os.path.exists(drv_src) and (force or _stale(exe, [drv_src, LIB, os.path.join(ROOT, "include", "amber_cuda.h")])):
             cc = shutil.which("gcc") or "cc"

@@ -647,11 +647,7 @@ int amber_cuda_calcr(amber_cuda_ctx *c, int max_tri, int *rcount, double *rdata)
     const int n = (int)tri.size() / 3;
     if ((rc = ensure(c, c->results, sizeof(double) * std::max(1, n), "calCR sums"))) return rc;
     c->last_ntri = 0;  // the sums below overwrite the last triangle run's lag arrays
-    const double *II = (const double *)c->maps_i.p;
-    for (int t = 0; t < n; ++t)
-        if ((rc = triple_sum(c, II + (long)tri[3 * t] * k, II + (long)tri[3 * t + 1] * k,
-                             II + (long)tri[3 * t + 2] * k, k, (double *)c->results.p + t)))
-            return rc;
+    if ((rc = triple_sums(c, (const double *)c->maps_i.p, k, tri, (double *)c->results.p))) return rc;
     std::vector<double> num(std::max(1, n));
     if ((rc = cuda_check(c, cudaMemcpyAsync(num.data(), c->results.p, sizeof(double) * n, cudaMemcpyDeviceToHost,
                                             c->stream),

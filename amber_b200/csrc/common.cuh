@@ -209,6 +209,7 @@ size_t contract_partial_cap(const amber_cuda_ctx *c);
 size_t cyl_bs_bytes(int nc10, int n_cut, int ntri);
 const char *cyl_bs_invalid(const amber_cuda_cylbs_params *p, int nc10, int have_mask_sums);
 // Σ_x a·b·c over n points (FP64, deterministic) into out[0].
-int triple_sum(amber_cuda_ctx *c, const double *a, const double *b, const double *cc, long n, double *out);
+// calCR: Num of every triangle (r1, r2, r3 in tri) from the N1² mask maps [ring][n], into device out[t].
+int triple_sums(amber_cuda_ctx *c, const double *maps, long n, const std::vector<int> &tri, double *out);
 
 }  // namespace amber

@@ -174,10 +174,20 @@ __global__ void lag_reduce_final(const double *__restrict__ part, int G, long nc
     lag[d] = s + comp;
 }
 
-__global__ void triple_sum_partial(const double *__restrict__ a, const double *__restrict__ b,
-                                   const double *__restrict__ c, long n, double *__restrict__ part)
+// calCR's Num for every closed triangle at once (amber_funcs.c:451-457):
+// Num_t = Σ_x II_r1(x)·II_r2(x)·II_r3(x) over the N1² mask maps.  CTA (chunk,
+// t) sums a fixed grid-stride slice of pixels; one thread per triangle then
+// adds the slices in order with compensation.  The grouping depends only on
+// the map size, so every triangle's Num is deterministic.
+constexpr int kNumChunks = 256;
+
+__global__ void triple_sum_partial(const double *__restrict__ maps, long n, const int *__restrict__ tri,
+                                   double *__restrict__ part)
 {
     __shared__ double red[256];
+    const int t = blockIdx.y;
+    const double *a = maps + (long)tri[3 * t] * n, *b = maps + (long)tri[3 * t + 1] * n,
+                 *c = maps + (long)tri[3 * t + 2] * n;
     double s = 0.0;
     for (long i = (long)blockIdx.x * 256 + threadIdx.x; i < n; i += (long)gridDim.x * 256) s += a[i] * b[i] * c[i];
     red[threadIdx.x] = s;
@@ -186,21 +196,22 @@ __global__ void triple_sum_partial(const double *__restrict__ a, const double *_
         if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
         __syncthreads();
     }
-    if (threadIdx.x == 0) part[blockIdx.x] = red[0];
+    if (threadIdx.x == 0) part[(long)t * gridDim.x + blockIdx.x] = red[0];
 }
 
-__global__ void sum_fixed(const double *__restrict__ part, int n, double *__restrict__ out)
+__global__ void sum_fixed(const double *__restrict__ part, int n, int ntri, double *__restrict__ out)
 {
-    if (threadIdx.x == 0 && blockIdx.x == 0) {
-        double s = 0.0, comp = 0.0;
-        for (int i = 0; i < n; ++i) {
-            double t = s + part[i];
-            double bp = t - s;
-            comp += (s - (t - bp)) + (part[i] - bp);
-            s = t;
-        }
-        out[0] = s + comp;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ntri) return;
+    const double *p = part + (long)t * n;
+    double s = 0.0, comp = 0.0;
+    for (int i = 0; i < n; ++i) {
+        double u = s + p[i];
+        double bp = u - s;
+        comp += (s - (u - bp)) + (p[i] - bp);
+        s = u;
     }
+    out[t] = s + comp;
 }
 
 }  // namespace
@@ -252,14 +263,28 @@ int contract_fp64(amber_cuda_ctx *c, const double *m1, const double *m2, const d
     return lag_reduce(c, (const double *)c->partial.p, (long)nA * KS, ncsize, lag_out);
 }
 
-int triple_sum(amber_cuda_ctx *c, const double *a, const double *b, const double *cc, long n, double *out)
+int triple_sums(amber_cuda_ctx *c, const double *maps, long n, const std::vector<int> &tri, double *out)
 {
-    const int nb = 256;
-    int rc = ensure(c, c->misc, sizeof(double) * nb, "triple-sum partials");
+    const int ntri = (int)tri.size() / 3;
+    if (ntri == 0) return AMBER_OK;
+    // partial sums [ntri][chunks] (doubles), then the triangle list (ints)
+    const size_t part_b = sizeof(double) * (size_t)ntri * kNumChunks;
+    int rc = ensure(c, c->misc, part_b + sizeof(int) * tri.size(), "calCR partial sums");
     if (rc) return rc;
-    triple_sum_partial<<<nb, 256, 0, c->stream>>>(a, b, cc, n, (double *)c->misc.p);
-    sum_fixed<<<1, 32, 0, c->stream>>>((const double *)c->misc.p, nb, out);
-    return cuda_check(c, cudaGetLastError(), "triple_sum launch");
+    double *part = (double *)c->misc.p;
+    int *d_tri = (int *)((char *)c->misc.p + part_b);
+    if ((rc = cuda_check(c, cudaMemcpyAsync(d_tri, tri.data(), sizeof(int) * tri.size(), cudaMemcpyHostToDevice,
+                                            c->stream), "calCR triangles")))
+        return rc;
+    for (int t0 = 0; t0 < ntri; t0 += 65535) {  // grid y limit
+        const int nt = std::min(65535, ntri - t0);
+        triple_sum_partial<<<dim3(kNumChunks, nt), 256, 0, c->stream>>>(maps, n, d_tri + 3 * t0,
+                                                                         part + (size_t)t0 * kNumChunks);
+        c->launches += 1;
+    }
+    sum_fixed<<<(ntri + 127) / 128, 128, 0, c->stream>>>(part, kNumChunks, ntri, out);
+    c->launches += 1;
+    return cuda_check(c, cudaGetLastError(), "calCR sums launch");
 }
 
 }  // namespace amber

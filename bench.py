@@ -334,6 +334,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--tri-subset", default="", help="comma-separated triangle indices (profiling runs only)")
+    ap.add_argument("--tile-n", type=int, default=0, choices=[0, 32, 64],
+                    help="fix the contraction's p3 tile width instead of the autotuner's choice (profiling runs: "
+                         "under a profiler the tuner's trial timings are not representative)")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble measurement")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving-stream measurement")
     ap.add_argument("--maps", action="store_true",
@@ -375,7 +378,7 @@ def main():
 
     real = synth.config2(seed=1 + rank)
     stream = torch.cuda.current_stream(dev)
-    est = amber_b200.Estimator(device=local, precision="mixed", stream=stream.cuda_stream)
+    est = amber_b200.Estimator(device=local, precision="mixed", stream=stream.cuda_stream, tile_n=args.tile_n)
     est.load_grid(real.gv, real.counts, real.du, real.flag_key)
     est.set_rings(real.ulow, real.uhigh)
     est.set_channels(real.nc10, real.uf_chans)

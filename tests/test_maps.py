@@ -90,3 +90,28 @@ def test_device_argument_errors():
         for bad in ((0, 1.0, 500.0), (15, 0.0, 500.0), (15, 5.0, 5.0)):
             with pytest.raises(amber_b200.AmberError):
                 est.cl_dnu(*bad)
+
+
+@pytest.mark.gpu
+def test_maps_driver_writes_the_reference_file(tmp_path):
+    """maps_gpu (the MAPS executable): maps.c's arguments and input_params in, results/cldnu out,
+    the same text the reference's cl_dnu loop writes (and the oracle's values formatted alike)."""
+    import subprocess
+    from amber_b200 import build
+    build.build()
+    real = synth.tiny(40, 10, seed=55, nbins=4, hi=18.0, flagged=[3])
+    data = tmp_path / "data"
+    real.write(str(data), 1)
+    (tmp_path / "input_params").write_text(
+        f"{real.gv.shape[0]}\t{real.du!r}\t154.255e6\t40.00e03\t1\t{real.gv.shape[2]}\t{data}\n")
+    p = subprocess.run([build.MAPS_DRIVER, "1", "GV_data_1"], capture_output=True, text=True, cwd=tmp_path)
+    assert p.returncode == 0, p.stderr
+    got = (tmp_path / "results" / "cldnu").read_text()
+    o = oracle.cl_dnu(real)
+    nc = real.gv.shape[2]
+    want = "".join(f"{i}\t{o['binu'][i]:e}\t{j}\t{o['cldnu'][i, j]:e}\t{o['numdnu'][j]:e}\t{o['num'][i]}\n"
+                   for i in range(15) for j in range(nc))
+    assert got == want
+    if oracle.ref_available():
+        _, txt = oracle.run_ref_maps(real, oracle.tmpdir())
+        assert open(txt).read() == got
