@@ -292,6 +292,45 @@ def config4_section(amber_b200, synth, dev, args):
             "generation_s": t_gen}
 
 
+def config1_section(amber_b200, synth, dev, reps=5):
+    """The reference's own CPU-runnable case, whole (128^2 grid, 32 channels, 8 bins 2-60, nc10=31,
+    all 46 closed triangles, v1): the C ABI from host buffers (grid upload, rings, channels, calCR,
+    every triangle, lag arrays back) against the reference's complete run on all host threads
+    (oracle/_ref/ref_amber_fast: its sources built unchanged with the production flags)."""
+    real = synth.config1()
+    out = {"workload": "config 1, whole run: 128^2 grid, 32 channels, 8 log bins 2-60, nc10=31, v1, 46 triangles"}
+    for prec in ("mixed", "fp64"):
+        with amber_b200.Estimator(device=dev, precision=prec) as est:
+            times, products = [], 0.0
+            for r in range(reps + 1):
+                t0 = time.perf_counter()
+                est.load_grid(real.gv, real.counts, real.du, real.flag_key)
+                est.set_rings(real.ulow, real.uhigh)
+                est.set_channels(real.nc10)
+                rd = est.calcr()
+                bl, nd, _ = est.triangles(rd[:, :3].astype(np.int32), want_v2=False)
+                if r:  # the first pass warms up (autotuner, allocations)
+                    times.append(time.perf_counter() - t0)
+                products = est.last_run_stats()[0]
+        out[prec] = {"wall_ms_median": 1e3 * float(np.median(times)), "triangles": int(len(rd)), "products": products,
+                     "value": products / float(np.median(times)), "unit": UNIT}
+    try:
+        import oracle
+        if oracle.ref_available():
+            wd = tempfile.mkdtemp(prefix="amber_c1_")
+            try:
+                st, _ = oracle.run_ref_amber(real, wd, version=1, fast=True, nthreads=os.cpu_count())
+            finally:
+                shutil.rmtree(wd, ignore_errors=True)
+            out["reference"] = {"total_s": st["total_s"], "accum_s": st["accum_s"], "maps_s": st["maps_s"],
+                                "threads": st["threads"], "products": st["products"],
+                                "value": st["products"] / st["total_s"], "unit": UNIT}
+            out["speedup_e2e_vs_reference_run"] = st["total_s"] / (out["mixed"]["wall_ms_median"] * 1e-3)
+    except Exception as e:  # the comparison is a report, not the measurement
+        out["reference_error"] = str(e)[:200]
+    return out
+
+
 def maps_section(amber_b200, synth, dev):
     """The MAPS two-point function (amber_cuda_cl_dnu; maps.c's 15 bins from 1 to 500) of the
     single-realisation grid, against the reference's own cl_dnu pair loop (oracle/_ref/ref_maps,
@@ -339,6 +378,8 @@ def main():
                          "under a profiler the tuner's trial timings are not representative)")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble measurement")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving-stream measurement")
+    ap.add_argument("--config1", action="store_true",
+                    help="measure the reference's whole CPU-runnable case (config 1) beside the reference's own run")
     ap.add_argument("--maps", action="store_true",
                     help="measure the MAPS two-point function (amber_cuda_cl_dnu) instead of the default step")
     ap.add_argument("--config4", action="store_true",
@@ -367,6 +408,13 @@ def main():
             print(json.dumps(dict(metric=METRIC, impl="amber_b200", n_gpus=1, higher_is_better=True,
                                   dtype="int8 tensor-core digits, int32 accumulate, fp64 reduce", data="synthetic",
                                   config={"workload": c4["workload"]}, **{k: v for k, v in c4.items() if k != "workload"})))
+        return 0
+
+    if args.config1:
+        if rank == 0:
+            c1 = config1_section(amber_b200, synth, local)
+            print(json.dumps(dict(metric=METRIC, impl="amber_b200", n_gpus=1, higher_is_better=True, data="synthetic",
+                                  config={"workload": c1["workload"]}, **{k: v for k, v in c1.items() if k != "workload"})))
         return 0
 
     if args.maps:
