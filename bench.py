@@ -324,8 +324,10 @@ def config1_section(amber_b200, synth, dev, reps=5):
                 shutil.rmtree(wd, ignore_errors=True)
             out["reference"] = {"total_s": st["total_s"], "accum_s": st["accum_s"], "maps_s": st["maps_s"],
                                 "threads": st["threads"], "products": st["products"],
-                                "value": st["products"] / st["total_s"], "unit": UNIT}
-            out["speedup_e2e_vs_reference_run"] = st["total_s"] / (out["mixed"]["wall_ms_median"] * 1e-3)
+                                "value_accum": st["products"] / st["accum_s"], "unit": UNIT,
+                                "note": "accum_s is the reference's own timer scope (amber.c:230,285); maps_s runs "
+                                        "its map builder on the oracle's FP64 DFT in place of FFTW, which is slower"}
+            out["speedup_vs_reference_accum"] = st["accum_s"] / (out["mixed"]["wall_ms_median"] * 1e-3)
     except Exception as e:  # the comparison is a report, not the measurement
         out["reference_error"] = str(e)[:200]
     return out
