@@ -1,0 +1,61 @@
+"""The drop-in executables' argument and input handling, before any GPU work (runs on CPU)."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import amber_b200
+from amber_b200 import build, formats, synth
+
+
+@pytest.fixture(scope="module")
+def exes():
+    build.build()
+    return build
+
+
+def _run(args, cwd):
+    return subprocess.run(args, capture_output=True, text=True, cwd=cwd)
+
+
+def test_vcg_usage_and_bad_keys(exes, tmp_path):
+    p = _run([exes.VCG_DRIVER], tmp_path)
+    assert p.returncode == 1 and "Usage" in p.stdout
+    p = _run([exes.VCG_DRIVER, "vis", "params", "GV", "2", "0", "1", "samp"], tmp_path)
+    assert p.returncode == 1 and "0 or 1" in p.stderr
+
+
+def test_vcg_rejects_a_file_that_is_not_visibilities(exes, tmp_path):
+    (tmp_path / "params").write_text("4\t20.0\t1480.73\t1.\n")
+    (tmp_path / "vis").write_bytes(b"NOTAVIS!" + bytes(64))
+    p = _run([exes.VCG_DRIVER, "vis", "params", "GV", "1", "0", "1", "samp"], tmp_path)
+    assert p.returncode == 1 and "not a visibility file" in p.stderr
+
+
+def test_vcg_rejects_more_channels_than_the_file_holds(exes, tmp_path):
+    randpar, data = synth.make_visibilities(16, 1.0254384902642049, 3, 20, 5, umax=8.0)
+    formats.write_vis(tmp_path / "vis", randpar, data, np.float32(synth.NU0), 40.0e3, 1.0)
+    (tmp_path / "params").write_text("5\t8.0\t1480.73\t1.\n")
+    p = _run([exes.VCG_DRIVER, "vis", "params", "GV", "1", "0", "1", "samp"], tmp_path)
+    assert p.returncode == 1 and "holds 3" in p.stderr
+
+
+def test_maps_usage_and_missing_inputs(exes, tmp_path):
+    p = _run([exes.MAPS_DRIVER], tmp_path)
+    assert p.returncode == 1 and "Usage" in p.stdout
+    p = _run([exes.MAPS_DRIVER, "1", "GV_data_1"], tmp_path)
+    assert p.returncode != 0 and "input_params" in p.stderr
+    (tmp_path / "input_params").write_text(f"32\t0.5\t154.255e6\t40e3\t1\t8\t{tmp_path / 'nowhere'}\n")
+    p = _run([exes.MAPS_DRIVER, "1", "GV_data_1"], tmp_path)
+    assert p.returncode != 0 and "GV_data" in p.stderr
+
+
+def test_cylbs_parameter_checks():
+    with pytest.raises(ValueError):
+        amber_b200.cylbs_params(denominator="both")
+    with pytest.raises(TypeError):
+        amber_b200.cylbs_params(n_kut=3)
+    p = amber_b200.cylbs_params(window=True, denominator="mask", n_cut=3)
+    assert (p.n_cut, p.window, p.denominator) == (3, 1, 1)
+    assert p.mabs_norm == amber_b200.reference_cylbs_constants()["mabs_norm"]
