@@ -168,3 +168,27 @@ def write_vis(path, randpar: np.ndarray, data: np.ndarray, nu_chan0: float, del_
             [randpar.astype(np.float32), data.astype(np.float32).reshape(g, -1)], axis=1
         )
         rec.tofile(f)
+
+
+def write_cldnu(path, cldnu: np.ndarray, numdnu: np.ndarray, binu: np.ndarray, num: np.ndarray) -> None:
+    """MAPS result file (4_fbe/maps.c:195-206): for every bin i and channel lag j one line
+    "i\tbinu[i]\tj\tcldnu[i][j]\tnumdnu[j]\tnum[i]" with C's %e for the reals."""
+    nb, nc = cldnu.shape
+    with open(path, "w") as f:
+        for i in range(nb):
+            for j in range(nc):
+                f.write(f"{i}\t{binu[i]:e}\t{j}\t{cldnu[i, j]:e}\t{numdnu[j]:e}\t{int(num[i])}\n")
+
+
+def read_cldnu(path):
+    """Parse a MAPS result file: (cldnu [nb, nc], numdnu [nc], binu [nb], num [nb]) at the
+    file's printed precision."""
+    rows = [ln.split("\t") for ln in open(path).read().splitlines() if ln.strip()]
+    nb = max(int(r[0]) for r in rows) + 1
+    nc = max(int(r[2]) for r in rows) + 1
+    cl, nd = np.zeros((nb, nc)), np.zeros(nc)
+    bu, nm = np.zeros(nb), np.zeros(nb, dtype=np.int64)
+    for r in rows:
+        i, j = int(r[0]), int(r[2])
+        bu[i], cl[i, j], nd[j], nm[i] = float(r[1]), float(r[3]), float(r[4]), int(r[5])
+    return cl, nd, bu, nm

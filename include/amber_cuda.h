@@ -164,7 +164,9 @@ AMBER_API int amber_cuda_cl_dnu(amber_cuda_ctx *ctx, int NB, double umin, double
  * tri_div (host, [ntri], may be NULL) divides each triangle's sums first: the v1
  * reader returns bldnu / Num (mabs_funcs.py:172-187), so pass Num for that chain.
  * out is [ntri][N][N] FP64 with N = 2·(nc10 + 1 − n_cut) − 1.  The reference
- * reads the lag arrays back from float files; here they are the FP64 sums. */
+ * reads the lag arrays back from float files; here they are the FP64 sums.
+ * n_cut = 0 keeps every cell (the reference's cut_nan(arr, 0) slices to an
+ * empty array, so it has no output to match there). */
 typedef struct amber_cuda_cylbs_params {
     int n_cut;        /* edge cells cut after folding (mabs_funcs.py n_nancut = 8) */
     int window;       /* 1: Blackman–Nuttall window, 0: none */

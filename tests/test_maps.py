@@ -115,3 +115,18 @@ def test_maps_driver_writes_the_reference_file(tmp_path):
     if oracle.ref_available():
         _, txt = oracle.run_ref_maps(real, oracle.tmpdir())
         assert open(txt).read() == got
+
+
+def test_cldnu_file_writer_matches_the_reference_text(tmp_path):
+    """formats.write_cldnu writes the reference's results/cldnu text (same %e formatting) from the
+    golden values; read_cldnu parses it back to the printed precision."""
+    from amber_b200 import formats
+    z, real = _golden()
+    p = tmp_path / "cldnu"
+    formats.write_cldnu(p, z["maps_cldnu"], z["maps_numdnu"], z["maps_binu"], z["maps_num"])
+    cl, nd, bu, nm = formats.read_cldnu(p)
+    np.testing.assert_allclose(cl, z["maps_cldnu"], rtol=1e-6, atol=1e-300)
+    np.testing.assert_array_equal(nm, z["maps_num"])
+    if oracle.ref_available():
+        _, txt = oracle.run_ref_maps(real, oracle.tmpdir())
+        assert open(txt).read() == p.read_text()
