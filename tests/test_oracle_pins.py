@@ -148,3 +148,22 @@ def test_oracle_gridding_matches_fresh_reference_vcg():
                                                 oracle.tmpdir())
     g2, n2 = oracle.grid_vis(nn_ref, nc, du_ref, umax, np.float32(synth.NU0), 1, randpar, data)
     assert np.array_equal(g2, gv) and np.array_equal(n2, nt)
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="reference build (oracle/_ref) not present")
+@pytest.mark.parametrize("nc,flag_key", [(8, 0), (11, 1)])
+def test_oracle_collapse_matches_fresh_reference_vcg(nc, flag_key):
+    """The reference's gridding stage run with the collapse key: 4 channels per output channel,
+    trailing channels dropped (11 → 2)."""
+    import math
+    fwhm, umax = 1480.73, 18.0
+    theta0 = 0.6 * fwhm * math.pi / (180. * 60.)
+    du = math.sqrt(math.log(2)) / (math.pi * theta0)
+    nn = 2 * int(math.ceil(umax / du))
+    randpar, data = synth.make_visibilities(nn, du, nc, 400, 70 + nc, umax=umax * 1.05)
+    gv, nt, du_ref, nn_ref = oracle.run_ref_vcg(randpar, data, np.float32(synth.NU0), nc, umax, fwhm, flag_key,
+                                                oracle.tmpdir(), collapse=True)
+    g, n = oracle.grid_vis(nn_ref, nc, du_ref, umax, np.float32(synth.NU0), flag_key, randpar, data)
+    g2, n2 = oracle.collapse_channels(g, n, 4)
+    assert gv.shape[2] == nc // 4
+    assert np.array_equal(g2, gv) and np.array_equal(n2, nt)
