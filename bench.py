@@ -333,6 +333,46 @@ def config1_section(amber_b200, synth, dev, reps=5):
     return out
 
 
+def stages_section(amber_b200, synth, dev, reps=5):
+    """The stages either side of the contraction, on the single-realisation workload: the
+    cylindrical bispectra of all 218 triangles after a v2 run (both analysis chains), and the
+    gridding of 100k visibility records (128 channels) without and with the 4-channel collapse.
+    Each figure is the median wall time of a synchronous C-ABI call, host copies included."""
+    real = synth.config2(seed=1)
+    res = {"workload": "stages beside the contraction: cylindrical bispectra of the single-realisation run "
+                       "(218 triangles, nc10=63, n_cut=8, N=111); gridding of 100k records x 128 channels "
+                       "onto the 256^2 grid"}
+
+    def med(f):
+        f()
+        ts = []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            f()
+            ts.append(time.perf_counter() - t0)
+        return 1e3 * float(np.median(ts))
+
+    with amber_b200.Estimator(device=dev, precision="mixed") as est:
+        est.load_grid(real.gv, real.counts, real.du, real.flag_key)
+        est.set_rings(real.ulow, real.uhigh)
+        est.set_channels(real.nc10, real.uf_chans)
+        rd = est.calcr()
+        est.run(rd[:, :3].astype(np.int32), want_v2=True)
+        num = est.file_num(rd)
+        res["cyl_bs_v1_ms"] = med(lambda: est.cyl_bs(tri_div=num))
+        res["cyl_bs_v2_window_ms"] = med(lambda: est.cyl_bs(window=True, denominator="mask"))
+        res["triangles"] = int(len(rd))
+        nn, du, nc = 256, 0.5, 128
+        randpar, data = synth.make_visibilities(nn, du, nc, 100000, 91)
+        umax = 0.95 * du * nn / 2
+        res["grid_ms"] = med(lambda: est.grid_vis(nn, nc, du, umax, np.float32(synth.NU0), 1, randpar, data))
+        res["grid_collapse4_ms"] = med(lambda: est.grid_vis(nn, nc, du, umax, np.float32(synth.NU0), 1, randpar, data,
+                                                            n_collapse=4))
+        res["records"] = int(len(randpar))
+        res["record_bytes"] = int(randpar.nbytes + data.nbytes)
+    return res
+
+
 def maps_section(amber_b200, synth, dev):
     """The MAPS two-point function (amber_cuda_cl_dnu; maps.c's 15 bins from 1 to 500) of the
     single-realisation grid, against the reference's own cl_dnu pair loop (oracle/_ref/ref_maps,
@@ -382,6 +422,8 @@ def main():
     ap.add_argument("--no-serving", action="store_true", help="skip the serving-stream measurement")
     ap.add_argument("--config1", action="store_true",
                     help="measure the reference's whole CPU-runnable case (config 1) beside the reference's own run")
+    ap.add_argument("--stages", action="store_true",
+                    help="time the stages beside the contraction (cylindrical bispectra, gridding with collapse)")
     ap.add_argument("--maps", action="store_true",
                     help="measure the MAPS two-point function (amber_cuda_cl_dnu) instead of the default step")
     ap.add_argument("--config4", action="store_true",
@@ -417,6 +459,13 @@ def main():
             c1 = config1_section(amber_b200, synth, local)
             print(json.dumps(dict(metric=METRIC, impl="amber_b200", n_gpus=1, higher_is_better=True, data="synthetic",
                                   config={"workload": c1["workload"]}, **{k: v for k, v in c1.items() if k != "workload"})))
+        return 0
+
+    if args.stages:
+        if rank == 0:
+            st = stages_section(amber_b200, synth, local)
+            print(json.dumps(dict(impl="amber_b200", n_gpus=1, data="synthetic", config={"workload": st["workload"]},
+                                  **{k: v for k, v in st.items() if k != "workload"})))
         return 0
 
     if args.maps:
