@@ -447,7 +447,7 @@ int amber_cuda_create(const amber_cuda_opts *opts, amber_cuda_ctx **out)
     c->precision = o.precision == AMBER_PREC_FP64_ABS ? AMBER_PREC_FP64 : o.precision;
     c->fp64_abs = o.precision == AMBER_PREC_FP64_ABS;
     c->chunk_px = o.chunk_px;
-    if (o.tile_n != 0 && o.tile_n != 32 && o.tile_n != 64) {
+    if (o.tile_n != 0 && o.tile_n != 32 && o.tile_n != 64 && o.tile_n != 128) {
         delete c;
         return AMBER_ERR_ARG;
     }

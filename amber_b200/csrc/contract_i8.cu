@@ -513,6 +513,325 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     }
 }
 
+// ---- 128-wide p3 tiles, both operands from shared memory (the SS MMA form) ----
+//
+// Four 128-column accumulators fill all 512 TMEM columns, so A cannot be staged in TMEM: the
+// MMAs read the D2 digit tiles straight from the TMA ring (64B-swizzled, K-major) and the B
+// digits from a 64B-swizzled ring the formers fill.  No movers.  A stage is 64 pixels (one D2
+// tile, two 32-pixel K slices): nine digit pairs × 2 slices = 18 MMAs of N = 128, each twice
+// the work of an N = 64 MMA for little more time.  The MMAs of a stage retire ~700 cycles
+// after they are issued, so the B ring needs three stages; to make room the fp32 inputs come in
+// 32-pixel half stages (one 128-row TMA box and the D1 row's 32 pixels each) through a ring of
+// three: formers of warps 0-7 take the first half of every stage, warps 8-15 the second.  The
+// digit arithmetic, the int32 classes and the epilogue are those of contract_i8_kernel, so
+// results are bit-identical to it.
+//
+// Warp roles (640 threads): warps 0-15 form the B digits and run the epilogue, warp 16 streams
+// the fp32 half stages, warp 17 owns TMEM and issues MMAs for accumulators 0 and 2, warp 18
+// streams the D2 digit tiles, warp 19 issues MMAs for accumulators 1 and 3.
+constexpr int SS_BN = 128;
+constexpr int SS_KB = 64;                      // pixels per stage
+constexpr int SS_HALF = 32;                    // pixels per fp32 half stage
+constexpr int SS_NBI = 3;                      // fp32 half stages in shared memory
+constexpr int SS_HALF_BYTES = SS_BN * SS_HALF * 4;  // one 128B-swizzled box of 128 rows
+constexpr int SS_NSB = 3;                      // B digit stages
+constexpr int SS_NAS = 3;                      // D2 digit tiles
+constexpr int SS_TILE = SS_BN * SS_KB;          // one B digit plane: 128 rows × 64 bytes
+constexpr int SS_STAGE_BD = NDB * SS_TILE;
+constexpr int SS_NWARP_B = 16;
+constexpr int SS_WARP_TMA = 16, SS_WARP_MMA = 17, SS_WARP_TMA_A = 18, SS_WARP_MMA2 = 19;
+constexpr int SS_NTHREADS = 20 * 32;
+
+// Shared-memory matrix descriptor: K-major, 64-byte swizzle, 8-row atoms of 512 B.
+__device__ __forceinline__ uint64_t smem_desc_sw64(uint32_t saddr)
+{
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFF);        // start address
+    d |= (uint64_t)(1) << 16;                       // leading byte offset (unused for swizzled K-major)
+    d |= (uint64_t)((512 >> 4) & 0x3FFF) << 32;    // stride byte offset: 8 rows × 64 B
+    d |= (uint64_t)1 << 46;                         // descriptor version (sm_100)
+    d |= (uint64_t)4 << 61;                         // SWIZZLE_64B
+    return d;
+}
+
+// kind::i8 MMA, A and B from shared memory
+__device__ __forceinline__ void umma_ss_i8(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
+                                           uint32_t accumulate)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
+// One issuer's share of a 64-pixel stage: accumulators k = q and q + 2, grouped by accumulator.
+__device__ __forceinline__ void issue_stage_ss(uint32_t tmem, uint64_t a_stage, uint64_t b_stage, uint32_t idesc,
+                                               int q, bool fresh)
+{
+    constexpr uint32_t A16 = (uint32_t)A_BOX >> 4, B16 = (uint32_t)SS_TILE >> 4;
+#pragma unroll
+    for (int kc = 0; kc < 2; ++kc) {
+        const int k = q + 2 * kc;
+        const uint32_t acc = tmem + (uint32_t)(k * SS_BN);
+        bool first = true;
+#pragma unroll
+        for (int kk = 0; kk < 2; ++kk)
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const int j = k - i;
+                if (j < 0 || j >= NDB) continue;
+                // K slice kk = bytes [32kk, 32kk+32) of each 64-byte row: +2 in 16-byte units
+                umma_ss_i8(acc, a_stage + (uint64_t)(i * A16 + kk * 2), b_stage + (uint64_t)(j * B16 + kk * 2), idesc,
+                           (first && fresh) ? 0u : 1u);
+                first = false;
+            }
+    }
+}
+
+__global__ void __launch_bounds__(SS_NTHREADS, 1)
+    contract_i8_ss_kernel(const JobDesc *__restrict__ jobs, const Item *__restrict__ items, int nitems, int *err)
+{
+    constexpr int BN = SS_BN;
+    constexpr int PT = BN * SS_KB / (SS_NWARP_B * 32);  // 16 pixels per former thread per stage
+    static_assert(PT == 16, "former pixels per thread");
+    static_assert(NACC * BN <= TMEM_COLS, "accumulators must fit in TMEM");
+    static_assert(NEPI == SS_NWARP_B, "the formers run the epilogue");
+
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    unsigned char *smem = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    unsigned char *bin = smem;                               // SS_NBI × SS_HALF_BYTES
+    unsigned char *bdig = bin + SS_NBI * SS_HALF_BYTES;      // SS_NSB × SS_STAGE_BD
+    unsigned char *atile = bdig + SS_NSB * SS_STAGE_BD;      // SS_NAS × 3 × A_BOX
+    float *d1rows = reinterpret_cast<float *>(atile + SS_NAS * 3 * A_BOX);  // SS_NBI × SS_HALF fp32
+    uint64_t *bars = reinterpret_cast<uint64_t *>(d1rows + SS_NBI * SS_HALF);
+    uint64_t *as_full = bars, *as_empty = as_full + SS_NAS;
+    uint64_t *bin_full = as_empty + SS_NAS, *bin_empty = bin_full + SS_NBI;
+    uint64_t *st_full = bin_empty + SS_NBI, *st_empty = st_full + SS_NSB;
+    uint64_t *acc_full = st_empty + SS_NSB, *acc_empty = acc_full + 1;
+    uint64_t *drain = acc_empty + 1;  // one per issuer
+    volatile uint32_t *tmem_slot = reinterpret_cast<volatile uint32_t *>(drain + NISSUE);
+    volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+    if (tid == 0) {
+        for (int s = 0; s < SS_NAS; ++s) { mbar_init(&as_full[s], 1); mbar_init(&as_empty[s], NISSUE); }
+        // a half stage is read by the 8 former warps of its half
+        for (int s = 0; s < SS_NBI; ++s) { mbar_init(&bin_full[s], 1); mbar_init(&bin_empty[s], SS_NWARP_B / 2); }
+        for (int s = 0; s < SS_NSB; ++s) { mbar_init(&st_full[s], SS_NWARP_B); mbar_init(&st_empty[s], NISSUE); }
+        mbar_init(acc_full, NISSUE);
+        mbar_init(acc_empty, NEPI);
+        for (int q = 0; q < NISSUE; ++q) mbar_init(&drain[q], 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == SS_WARP_MMA) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32((const void *)tmem_slot)),
+                     "r"(TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    fence_before();
+    __syncthreads();
+    fence_after();
+    const uint32_t tmem = *tmem_slot;
+    bool ok = true;
+    // 64-pixel stages of an item
+    auto stages_of = [&](const ItemView &v) {
+        const long x_end = min(v.j->k, v.x_begin + v.j->chunk);
+        return (int)((x_end - v.x_begin + SS_KB - 1) / SS_KB);
+    };
+
+    if (warp == SS_WARP_TMA) {
+        // fp32 half stages: D3 rows [bbase, bbase+128) × 32 pixels (128B-swizzled) and the D1 row's
+        // 32 pixels; pixels past the end of the map and rows outside [0, nc) come back as zeros
+        if (lane == 0) {
+            int gh = 0;  // half stages issued so far
+            for (int g = blockIdx.x; g < nitems && ok; g += gridDim.x) {
+                const ItemView v = decode<BN>(jobs, items, g);
+                const int nh = 2 * stages_of(v);
+                for (int ih = 0; ih < nh; ++ih, ++gh) {
+                    const int s = gh % SS_NBI;
+                    if (!mbar_wait(&bin_empty[s], ((gh / SS_NBI) & 1) ^ 1, abort_flag, err, 11)) { ok = false; break; }
+                    mbar_expect_tx(&bin_full[s], SS_HALF_BYTES + SS_HALF * 4);
+                    const int x = (int)(v.x_begin + (long)ih * SS_HALF);
+                    tma_load_2d(bin + s * SS_HALF_BYTES, &v.j->td3, &bin_full[s], x, v.bbase);
+                    tma_load_2d(d1rows + s * SS_HALF, &v.j->td1, &bin_full[s], x, v.p1);
+                }
+            }
+            if (!ok)
+                for (int q = max(0, gh - SS_NBI); q < gh; ++q)
+                    for (long long i = 0; i < WAIT_LIMIT && !mbar_try_wait(&bin_full[q % SS_NBI], ((q / SS_NBI) & 1)); ++i)
+                        __nanosleep(100);
+        }
+    } else if (warp == SS_WARP_TMA_A) {
+        // D2 digit planes, rows [rbase, rbase+128) × 64 pixels: one tile per stage; rows outside
+        // [0, nc) and pixels past the end of the map come back as zeros
+        if (lane == 0) {
+            int gs = 0;
+            for (int g = blockIdx.x; g < nitems && ok; g += gridDim.x) {
+                const ItemView v = decode<BN>(jobs, items, g);
+                const int nb = stages_of(v);
+                for (int it = 0; it < nb; ++it, ++gs) {
+                    const int s = gs % SS_NAS;
+                    if (!mbar_wait(&as_empty[s], ((gs / SS_NAS) & 1) ^ 1, abort_flag, err, 18)) { ok = false; break; }
+                    unsigned char *t = atile + s * 3 * A_BOX;
+                    mbar_expect_tx(&as_full[s], 3 * A_BOX);
+                    const int x = (int)(v.x_begin + (long)it * SS_KB);
+                    tma_load_2d(t, &v.j->ta[0], &as_full[s], x, v.rbase);
+                    tma_load_2d(t + A_BOX, &v.j->ta[1], &as_full[s], x, v.rbase);
+                    tma_load_2d(t + 2 * A_BOX, &v.j->ta[2], &as_full[s], x, v.rbase);
+                }
+            }
+            if (!ok)
+                for (int q = max(0, gs - SS_NAS); q < gs; ++q)
+                    for (long long i = 0; i < WAIT_LIMIT && !mbar_try_wait(&as_full[q % SS_NAS], ((q / SS_NAS) & 1)); ++i)
+                        __nanosleep(100);
+        }
+    } else if (warp == SS_WARP_MMA || warp == SS_WARP_MMA2) {
+        if (lane == 0) {
+            const int q = warp == SS_WARP_MMA ? 0 : 1;
+            // S32 accumulate, signed int8 A and B, both K-major, M = 128, N = 128
+            const uint32_t idesc = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
+                                   ((uint32_t)(BM >> 4) << 24);
+            // descriptors are linear in the start address (bits 0-13, 16-byte units)
+            const uint64_t adesc0 = smem_desc_sw64(smem_u32(atile));
+            const uint64_t bdesc0 = smem_desc_sw64(smem_u32(bdig));
+            int gs = 0, seq = 0;
+            for (int g = blockIdx.x; g < nitems && ok; g += gridDim.x, ++seq) {
+                const int nb = stages_of(decode<BN>(jobs, items, g));
+                if (!mbar_wait(acc_empty, (seq & 1) ^ 1, abort_flag, err, 20)) { ok = false; break; }
+                for (int it = 0; it < nb; ++it, ++gs) {
+                    const int s = gs % SS_NSB, sa = gs % SS_NAS;
+                    if (!mbar_wait(&st_full[s], ((gs / SS_NSB) & 1), abort_flag, err, 12)) { ok = false; break; }
+                    if (!mbar_wait(&as_full[sa], ((gs / SS_NAS) & 1), abort_flag, err, 19)) { ok = false; break; }
+                    fence_after();
+                    issue_stage_ss(tmem, adesc0 + (uint64_t)((sa * 3 * A_BOX) >> 4),
+                                   bdesc0 + (uint64_t)((s * SS_STAGE_BD) >> 4), idesc, q, it == 0);
+                    umma_commit(&st_empty[s]);
+                    umma_commit(&as_empty[sa]);
+                }
+                if (ok) umma_commit(acc_full);
+            }
+            if (!ok) {
+                umma_commit(&drain[q]);
+                for (long long i = 0; i < WAIT_LIMIT && !mbar_try_wait(&drain[q], 0); ++i) __nanosleep(100);
+            }
+        }
+    } else {
+        // ---- warps 0-15: B formers, then each item's epilogue ----
+        const uint32_t lane_field = (uint32_t)((warp & 3) << 5) << 16;
+        // thread (row n, segment sg) forms pixels 16sg .. 16sg+15 of D1[p1]·D3[bbase+n] per stage:
+        // segments 0-1 (warps 0-7) read the stage's first fp32 half, segments 2-3 the second
+        const int n = tid % BN, sg = tid / BN;
+        const int half = sg >> 1;
+        const int c0 = (sg & 1) * 4;  // first 16-byte chunk of the thread's 16 pixels in the half's 128-byte row
+        // destination: 16-byte chunk sg of each 64-byte digit row, at its 64B-swizzled position
+        const int dst_off = n * SS_KB + ((sg ^ ((n >> 1) & 3)) << 4);
+        int gs = 0, seq = 0;
+        for (int g = blockIdx.x; g < nitems && ok; g += gridDim.x, ++seq) {
+            const ItemView v = decode<BN>(jobs, items, g);
+            const JobDesc &j = *v.j;
+            const int nb = stages_of(v);
+            const int p3 = v.bbase + n;
+            const bool col_ok = p3 >= 0 && p3 < j.nc;
+            const float scale = col_ok ? ldexpf(127.f, -(v.E1 + j.e3[p3])) : 0.f;
+            const float2 sc2 = make_float2(scale, scale);
+            for (int it = 0; it < nb; ++it, ++gs) {
+                const int gh = 2 * gs + half;  // this thread's half stage
+                const int si = gh % SS_NBI, s = gs % SS_NSB;
+                if (!mbar_wait_warp(&bin_full[si], ((gh / SS_NBI) & 1), abort_flag, err, 16)) { ok = false; break; }
+                const unsigned char *rowp = bin + si * SS_HALF_BYTES + n * 128;
+                const float *d1p = d1rows + si * SS_HALF + (sg & 1) * 16;
+                uint32_t w[NDB][PT / 4];
+#pragma unroll
+                for (int qq = 0; qq < PT / 4; ++qq) {
+                    const float4 x3 = *reinterpret_cast<const float4 *>(rowp + (((c0 + qq) ^ (n & 7)) << 4));
+                    const float4 u = *reinterpret_cast<const float4 *>(d1p + 4 * qq);
+                    float2 ya0, ya1, ya2, ya3, yb0, yb1, yb2, yb3;
+                    digits254x2(__fmul2_rn(make_float2(u.x, u.y), sc2), make_float2(x3.x, x3.y), ya0, ya1, ya2, ya3);
+                    digits254x2(__fmul2_rn(make_float2(u.z, u.w), sc2), make_float2(x3.z, x3.w), yb0, yb1, yb2, yb3);
+                    w[0][qq] = pack_low_bytes(ya0.x, ya0.y, yb0.x, yb0.y);
+                    w[1][qq] = pack_low_bytes(ya1.x, ya1.y, yb1.x, yb1.y);
+                    w[2][qq] = pack_low_bytes(ya2.x, ya2.y, yb2.x, yb2.y);
+                    w[3][qq] = pack_low_bytes(ya3.x, ya3.y, yb3.x, yb3.y);
+                }
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&bin_empty[si]);
+                if (!mbar_wait_warp(&st_empty[s], ((gs / SS_NSB) & 1) ^ 1, abort_flag, err, 17)) { ok = false; break; }
+                unsigned char *dst = bdig + s * SS_STAGE_BD + dst_off;
+#pragma unroll
+                for (int d = 0; d < NDB; ++d)
+                    *reinterpret_cast<uint4 *>(dst + d * SS_TILE) = make_uint4(w[d][0], w[d][1], w[d][2], w[d][3]);
+                fence_proxy_async_smem();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&st_full[s]);
+            }
+            // ---- epilogue: int32 digit accumulators → FP64 partial tile; warpgroup wg reads BN/4 columns ----
+            const int wg = warp >> 2;
+            const int me = ((warp & 3) << 5) + lane;
+            const bool good = __all_sync(0xffffffffu, ok) && mbar_wait_warp(acc_full, (seq & 1), abort_flag, err, 15);
+            if (!good) { ok = false; break; }
+            fence_after();
+            const int d2 = v.mt * BM + me;
+            const int p2 = v.rbase + me;
+            const bool row_ok = d2 < j.nclen && p2 >= 0 && p2 < j.nc && j.weight[p2] > 0;
+            const int E12 = v.E1 + (row_ok ? j.e2[p2] : 0);
+            const double wr = row_ok ? (double)j.weight[v.p1] * (double)j.weight[p2] : 0.0;
+            double *dst = nullptr;
+            if (d2 < j.nclen)
+                dst = j.partial + ((long)v.aidx * j.nchunk + v.chunk) * j.nclen * j.nclen + (long)d2 * j.nclen;
+            const int c_begin = wg * (BN / 4), c_end = c_begin + BN / 4;
+            const double i254 = 1.0 / 254.0, i254_2 = i254 * i254, i254_3 = i254_2 * i254;
+            for (int cb = c_begin; cb < c_end; cb += 8) {
+                uint32_t v0[8], v1[8], v2[8], v3[8];
+                tmem_ld8(tmem + lane_field + cb, v0);
+                tmem_ld8(tmem + lane_field + BN + cb, v1);
+                tmem_ld8(tmem + lane_field + 2 * BN + cb, v2);
+                tmem_ld8(tmem + lane_field + 3 * BN + cb, v3);
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                if (cb + 8 >= c_end) {
+                    // last read of this item: hand the accumulators back to the MMA issuers
+                    fence_before();
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(acc_empty);
+                }
+                if (dst) {
+#pragma unroll
+                    for (int e = 0; e < 8; ++e) {
+                        const int nn = cb + e;
+                        const int d3 = v.nt * BN + nn;
+                        if (d3 >= j.nclen) continue;
+                        const int q3 = v.bbase + nn;
+                        double val = 0.0;
+                        if (wr != 0.0 && q3 >= 0 && q3 < j.nc && j.weight[q3] > 0) {
+                            const double sm = (double)(int)v0[e] + (double)(int)v1[e] * i254 +
+                                              (double)(int)v2[e] * i254_2 + (double)(int)v3[e] * i254_3;
+                            val = ldexp(sm * (1.0 / 16129.0), E12 + j.e3[q3]) * wr * (double)j.weight[q3];
+                        }
+                        dst[d3] = val;
+                    }
+                }
+            }
+        }
+    }
+
+    fence_before();
+    __syncthreads();
+    if (warp == SS_WARP_MMA) {
+        fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
+    }
+}
+
+size_t smem_bytes_ss()
+{
+    return 1024 + (size_t)SS_NBI * SS_HALF_BYTES + (size_t)SS_NSB * SS_STAGE_BD + (size_t)SS_NAS * 3 * A_BOX +
+           (size_t)SS_NBI * SS_HALF * 4 + 256;
+}
+
 template <int BN>
 size_t smem_bytes()
 {
@@ -578,6 +897,17 @@ struct Planned {
     bool accumulate;  // a later anchor group of a split job: its lag sum adds to the array
 };
 
+int launch_ss(amber_cuda_ctx *c, const JobDesc *d_jobs, const Item *d_items, long nitems, long grid_ctas, int *d_err)
+{
+    const size_t sm = smem_bytes_ss();
+    cudaFuncSetAttribute(contract_i8_ss_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    const unsigned grid = (unsigned)std::min<long>(nitems, grid_ctas);
+    contract_i8_ss_kernel<<<grid, SS_NTHREADS, sm, c->stream>>>(d_jobs, d_items, (int)nitems, d_err);
+    c->launches += 1;
+    c->contractions += 1;
+    return cuda_check(c, cudaGetLastError(), "contract_i8_ss_kernel launch");
+}
+
 template <int BN>
 int launch(amber_cuda_ctx *c, const JobDesc *d_jobs, const Item *d_items, long nitems, long grid_ctas, int *d_err)
 {
@@ -619,7 +949,9 @@ int fill_launch(amber_cuda_ctx *c, LaunchPlan &lp, char *stage, bool first_chunk
                 return rc;
         if ((rc = encode(c, &d.td3, f32, jb.m3.f32, jb.k, jb.kp * 4, jb.nc, 32, BN, CU_TENSOR_MAP_SWIZZLE_128B)))
             return rc;
-        if ((rc = encode(c, &d.td1, f32, jb.m1.f32, jb.k, jb.kp * 4, jb.nc, KB_B, 1, CU_TENSOR_MAP_SWIZZLE_NONE)))
+        // the D1 row: one box per stage (128 pixels; 32 for the 128-wide tiles' half stages)
+        if ((rc = encode(c, &d.td1, f32, jb.m1.f32, jb.k, jb.kp * 4, jb.nc, BN == SS_BN ? SS_HALF : KB_B, 1,
+                         CU_TENSOR_MAP_SWIZZLE_NONE)))
             return rc;
         d.e1 = jb.m1.expo; d.e2 = jb.m2.expo; d.e3 = jb.m3.expo;
         d.anchors = jb.anchors;
@@ -661,7 +993,7 @@ int execute_jobs(amber_cuda_ctx *c, const std::vector<const I8Job *> &jobs, cons
     const long big_items = 4L * c->num_sms;
     std::vector<LaunchPlan> plans;
     std::deque<I8Job> parts;  // anchor groups of jobs whose partial tiles exceed the cap
-    for (int BN : {32, 64}) {
+    for (int BN : {32, 64, SS_BN}) {
         LaunchPlan shared;
         for (size_t ji = 0; ji < jobs.size(); ++ji) {
             const I8Job &jb = *jobs[ji];
@@ -765,8 +1097,10 @@ int execute_jobs(amber_cuda_ctx *c, const std::vector<const I8Job *> &jobs, cons
         const Item *d_items = (const Item *)((char *)c->jobdesc.p + lp.item_off);
         phase_begin(c, 1);
         const long grid = lp.persistent ? c->num_sms : lp.nitems;
-        rc = lp.jobs[0].bn == 32 ? launch<32>(c, d_jobs, d_items, lp.nitems, grid, d_err)
-                                 : launch<64>(c, d_jobs, d_items, lp.nitems, grid, d_err);
+        const int bw = lp.jobs[0].bn;
+        rc = bw == 32   ? launch<32>(c, d_jobs, d_items, lp.nitems, grid, d_err)
+             : bw == 64 ? launch<64>(c, d_jobs, d_items, lp.nitems, grid, d_err)
+                        : launch_ss(c, d_jobs, d_items, lp.nitems, grid, d_err);
         phase_end(c);
         if (rc) return rc;
         if (first_chunk_only) continue;  // a timing trial: its partial tiles are not reduced
@@ -808,7 +1142,8 @@ int contract_i8_jobs(amber_cuda_ctx *c, const std::vector<I8Job> &jobs)
     for (const I8Job &jb : jobs) {
         const int nclen = 2 * jb.nc10 + 1;
         int w = nclen <= 32 ? 32 : 64;
-        if (c->tile_n && nclen <= 128) w = nclen <= 32 ? 32 : c->tile_n;
+        if (c->tile_n == SS_BN) w = SS_BN;
+        else if (c->tile_n && nclen <= 128) w = nclen <= 32 ? 32 : c->tile_n;
         if (!c->tile_n && nclen > 32 && nclen <= 128 && jb.nanchors > 0) {
             const int cls = tile_class(nclen);
             int known = 0;

@@ -415,7 +415,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--tri-subset", default="", help="comma-separated triangle indices (profiling runs only)")
-    ap.add_argument("--tile-n", type=int, default=0, choices=[0, 32, 64],
+    ap.add_argument("--tile-n", type=int, default=0, choices=[0, 32, 64, 128],
                     help="fix the contraction's p3 tile width instead of the autotuner's choice (profiling runs: "
                          "under a profiler the tuner's trial timings are not representative)")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble measurement")

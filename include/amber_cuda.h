@@ -54,8 +54,9 @@ typedef struct amber_cuda_opts {
     size_t hbm_budget;     /* max device bytes the context may hold; 0 = 90 % of free memory */
     void *stream;          /* optional cudaStream_t to launch on (NULL = the context's own stream) */
     int chunk_px;          /* tensor-core paths: pixels per CTA accumulation chunk before the FP64 flush (0 = default) */
-    int tile_n;            /* mixed path: p3 tile width 32 or 64; 0 = chosen by the autotuner (measured once per
-                              lag-window class and context).  Results do not depend on it. */
+    int tile_n;            /* mixed path: p3 tile width 32, 64 or 128 (128: both MMA operands from shared
+                              memory, N = 128); 0 = chosen by the autotuner (measured once per lag-window
+                              class and context).  Results do not depend on it. */
 } amber_cuda_opts;
 
 AMBER_API void amber_cuda_default_opts(amber_cuda_opts *opts);

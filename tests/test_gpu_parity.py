@@ -157,6 +157,24 @@ def test_tile_width_is_numerically_neutral(lib_built):
             np.testing.assert_array_equal(a, b)
 
 
+def test_ss_tile_is_bit_identical(lib_built):
+    """tile_n = 128 runs the contraction with both MMA operands in shared memory (N = 128, 64-pixel
+    stages): the same digit arithmetic and chunking, so its lag arrays equal the 64-wide path's bit
+    for bit — one tile (nclen = 39) and a 2 × 2 tile grid (nclen = 141, rows and pixels past the
+    ends, flagged channels)."""
+    import amber_b200
+    cases = [synth.tiny(64, 40, seed=52, nbins=6, hi=28.0, nc10=19, flagged=[0, 39]),
+             synth.tiny(96, 150, seed=53, nbins=5, hi=40.0, nc10=70, flagged=[3, 77, 149])]
+    for real in cases:
+        outs = []
+        for tile_n in (64, 128):
+            with amber_b200.Estimator(precision="mixed", tile_n=tile_n) as est:
+                amber_b200.estimate(real, precision="mixed", version=2, est=est)
+                outs.append(est.fetch(want_v2=True))
+        for a, b in zip(*outs):
+            np.testing.assert_array_equal(a, b)
+
+
 @pytest.mark.skipif(not oracle.ref_available(), reason="reference build (oracle/_ref) not present")
 def test_config1_full_vs_reference_build(tmp_path, lib_built):
     """The reference's own CPU-runnable case at full size (128² grid, 32 channels, 8 bins, all 46
