@@ -55,6 +55,10 @@
 // TMEM); warps 0-15 read the accumulators out.
 // Every mbarrier wait is bounded; on expiry the CTA raises an error flag the
 // host turns into AMBER_ERR_TIMEOUT, drains its own copies and MMAs, frees TMEM.
+//
+// contract_i8_ss_kernel (below) is the 128-wide variant with both MMA operands in
+// shared memory (tile_n = 128); it computes bit-identical results and is chosen
+// only on request.
 #include <algorithm>
 #include <cmath>
 #include <deque>
