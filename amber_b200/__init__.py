@@ -170,7 +170,15 @@ def _ptr(a, t):
 
 
 class Estimator:
-    """One libamber_cuda context (one device, one host thread)."""
+    """One libamber_cuda context (one device, one host thread).
+
+    precision: "mixed" (int8 tensor-core digits, ≤1e-6 of Σ|products| per lag cell), "fp64"
+    (plain FP64, ≤1e-10), "fp64_abs" (FP64 over |maps|: the error scale) or "bf16x3"
+    (comparison only).  hbm_budget: bytes the context may hold (0: most of the free memory).
+    stream: a cudaStream_t to launch on.  chunk_px: pixels per accumulation chunk (0: planned).
+    tile_n: the contraction's p3 tile width, 32, 64 or 128 (0: the autotuner's choice); results
+    do not depend on it.  Every call raises AmberError with the library's message on failure.
+    """
 
     def __init__(self, device: int = 0, precision: str = "mixed", hbm_budget: int = 0, stream: int | None = None,
                  chunk_px: int = 0, tile_n: int = 0):
