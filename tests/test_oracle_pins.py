@@ -132,7 +132,9 @@ def test_oracle_matches_fresh_reference_run(seed, flagged):
     for r in res:
         inv, bl, nd = formats.read_bsout_v2(os.path.join(rp, formats.bsout_name(2, r["r1"], r["r2"], r["r3"], 1)),
                                             real.nclen, np.float64)
-        assert np.abs(bl - r["bldnu"]).max() <= 1e-10 * r["absscale"].max()
+        # per lag cell, against Σ|products| of that cell; the v2 file's second array is the mask sums
+        assert (np.abs(bl - r["bldnu"]) <= 1e-10 * r["absscale"] + 1e-300).all()
+        assert (np.abs(nd - r["numtri"]) <= 1e-10 * r["absscale_i"] + 1e-300).all()
         assert inv == 1.0 / (r["ng1"] ** 2)
 
 
@@ -167,3 +169,27 @@ def test_oracle_collapse_matches_fresh_reference_vcg(nc, flag_key):
     g2, n2 = oracle.collapse_channels(g, n, 4)
     assert gv.shape[2] == nc // 4
     assert np.array_equal(g2, gv) and np.array_equal(n2, nt)
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="reference build (oracle/_ref) not present")
+@pytest.mark.parametrize("nn,nc,seed,nc10,flagged", [
+    (32, 6, 23, 0, None),                        # only the zero lag
+    (32, 7, 24, 6, None),                        # nc10 = nc - 1: the widest window
+    (36, 12, 25, 5, [0, 1, 2, 4, 6, 7, 9, 11]),  # most channels flagged
+])
+def test_oracle_matches_reference_at_edges(nn, nc, seed, nc10, flagged):
+    """The FP64 reference build (v1 files) against the oracle per lag cell at the edges of the
+    lag window and of the flag set: triangle list, counts exact, lag sums within 1e-10 of
+    Σ|products| of the same cell, the file scalars Num and Ntri."""
+    real = synth.tiny(nn, nc, seed=seed, nbins=3, hi=0.44 * nn, nc10=nc10, flagged=flagged)
+    st, rp = oracle.run_ref_amber(real, oracle.tmpdir(), version=1, fp64=True)
+    rdata, res = oracle.estimate(real, version=1, with_absscale=True)
+    np.testing.assert_array_equal(formats.read_closed_rings(rp)[:, :3], rdata[:, :3])
+    assert len(res) > 0
+    for r in res:
+        ntri, num, bl, nd = formats.read_bsout_v1(
+            os.path.join(rp, formats.bsout_name(1, r["r1"], r["r2"], r["r3"], 1)), real.nclen, bl_dtype=np.float64)
+        np.testing.assert_array_equal(nd, r["numdnu"])
+        assert (np.abs(bl - r["bldnu"]) <= 1e-10 * r["absscale"] + 1e-300).all()
+        np.testing.assert_allclose(num, (r["ng1"] / real.nn) ** 2 * r["rdata_num"], rtol=1e-12)
+        np.testing.assert_allclose(ntri, num / r["ng1"] ** 2, rtol=1e-12)
