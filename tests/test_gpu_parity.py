@@ -66,6 +66,8 @@ def test_estimator_vs_reference_golden(path, precision, lib_built):
     (48, 16, 5, 22.0, 7, None, 31),
     (64, 20, 6, 30.0, 9, [0, 1, 18, 19], 32),
     (56, 12, 4, 26.0, 11, [3], 33),  # nc10 = nc - 1: the widest lag window
+    (32, 6, 3, 14.0, 0, None, 34),  # nc10 = 0: the zero lag only
+    (36, 12, 3, 16.0, 5, [0, 1, 2, 4, 6, 7, 9, 11], 35),  # most channels flagged
 ])
 def test_estimator_vs_oracle(precision, nn, nc, nbins, hi, nc10, flagged, seed, lib_built):
     import amber_b200
