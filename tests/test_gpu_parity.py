@@ -262,6 +262,20 @@ def test_gridding_bit_exact_vs_reference(path, lib_built):
     assert np.array_equal(nt, z["ntig"])
 
 
+def test_gridding_edges(lib_built):
+    """No records at all (an all-zero grid), and a collapse of every channel into one."""
+    import amber_b200
+    nn, du, nc = 32, 0.5, 8
+    randpar, data = synth.make_visibilities(nn, du, nc, 400, 78)
+    nu0 = np.float32(synth.NU0)
+    with amber_b200.Estimator() as est:
+        g, n = est.grid_vis(nn, nc, du, 7.0, nu0, 1, randpar[:0], data[:0])
+        assert g.shape == (nn, nn // 2 + 1, nc) and not g.any() and not n.any()
+        g1, n1 = est.grid_vis(nn, nc, du, 7.0, nu0, 0, randpar, data, n_collapse=nc)
+    g_o, n_o = oracle.collapse_channels(*oracle.grid_vis(nn, nc, du, 7.0, nu0, 0, randpar, data), nc)
+    assert g1.shape[2] == 1 and np.array_equal(g1, g_o) and np.array_equal(n1, n_o)
+
+
 def test_gridding_bit_exact_vs_oracle_large(lib_built):
     import amber_b200
     nn, du, nc = 128, 0.5, 24

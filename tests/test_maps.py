@@ -130,3 +130,14 @@ def test_cldnu_file_writer_matches_the_reference_text(tmp_path):
     if oracle.ref_available():
         _, txt = oracle.run_ref_maps(real, oracle.tmpdir())
         assert open(txt).read() == p.read_text()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("bins", [(1, 1.0, 500.0), (6, 400.0, 500.0)])
+def test_device_single_bin_and_empty_bins(bins):
+    """One bin for every cell, and bins beyond the grid (no cell in any bin: all zeros)."""
+    real = synth.tiny(40, 9, seed=56, nbins=4, hi=18.0)
+    got = _device(real, *bins)
+    want = oracle.cl_dnu(real, *bins)
+    for k in KEYS:
+        np.testing.assert_array_equal(got[k], want[k], err_msg=k)
