@@ -165,12 +165,14 @@ def test_ss_tile_is_bit_identical(lib_built):
     for bit — one tile (nclen = 39) and a 2 × 2 tile grid (nclen = 141, rows and pixels past the
     ends, flagged channels)."""
     import amber_b200
-    cases = [synth.tiny(64, 40, seed=52, nbins=6, hi=28.0, nc10=19, flagged=[0, 39]),
-             synth.tiny(96, 150, seed=53, nbins=5, hi=40.0, nc10=70, flagged=[3, 77, 149])]
-    for real in cases:
+    cases = [(synth.tiny(64, 40, seed=52, nbins=6, hi=28.0, nc10=19, flagged=[0, 39]), 0),
+             (synth.tiny(96, 150, seed=53, nbins=5, hi=40.0, nc10=70, flagged=[3, 77, 149]), 0),
+             (synth.tiny(32, 10, seed=54, nbins=4, hi=14.0, nc10=4), 0),     # nclen = 9: mostly idle columns
+             (synth.tiny(64, 40, seed=55, nbins=6, hi=28.0, nc10=19), 128)]  # 128-pixel chunks, ragged last
+    for real, chunk_px in cases:
         outs = []
         for tile_n in (64, 128):
-            with amber_b200.Estimator(precision="mixed", tile_n=tile_n) as est:
+            with amber_b200.Estimator(precision="mixed", tile_n=tile_n, chunk_px=chunk_px) as est:
                 amber_b200.estimate(real, precision="mixed", version=2, est=est)
                 outs.append(est.fetch(want_v2=True))
         for a, b in zip(*outs):
