@@ -538,10 +538,13 @@ constexpr int SS_KB = 64;                      // pixels per stage
 constexpr int SS_HALF = 32;                    // pixels per fp32 half stage
 constexpr int SS_NBI = 3;                      // fp32 half stages in shared memory
 constexpr int SS_HALF_BYTES = SS_BN * SS_HALF * 4;  // one 128B-swizzled box of 128 rows
-constexpr int SS_NSB = 3;                      // B digit stages
-constexpr int SS_NAS = 3;                      // D2 digit tiles
-constexpr int SS_TILE = SS_BN * SS_KB;          // one B digit plane: 128 rows × 64 bytes
-constexpr int SS_STAGE_BD = NDB * SS_TILE;
+constexpr int SS_NSB = 4;                      // B digit stages: two 128-pixel slots, two stages each
+constexpr int SS_NAS = 2;                      // D2 digit tiles
+// B digits: 128-byte rows (128B swizzle, the fast layout for the MMA's reads), so a slot holds
+// two 64-pixel stages side by side in every row: stage gs fills bytes 64(gs & 1) .. +63 of slot
+// (gs / 2) % 2.
+constexpr int SS_PLANE = SS_BN * 128;           // one B digit plane of a slot: 128 rows × 128 bytes
+constexpr int SS_SLOT = NDB * SS_PLANE;         // 64 KB
 constexpr int SS_NWARP_B = 16;
 constexpr int SS_WARP_TMA = 16, SS_WARP_MMA = 17, SS_WARP_TMA_A = 18, SS_WARP_MMA2 = 19;
 constexpr int SS_NTHREADS = 20 * 32;
@@ -571,10 +574,12 @@ __device__ __forceinline__ void umma_ss_i8(uint32_t d_tmem, uint64_t a_desc, uin
 }
 
 // One issuer's share of a 64-pixel stage: accumulators k = q and q + 2, grouped by accumulator.
+// b_stage points at the stage's half of its slot (the start address already advanced by 64 bytes
+// for the second half).
 __device__ __forceinline__ void issue_stage_ss(uint32_t tmem, uint64_t a_stage, uint64_t b_stage, uint32_t idesc,
                                                int q, bool fresh)
 {
-    constexpr uint32_t A16 = (uint32_t)A_BOX >> 4, B16 = (uint32_t)SS_TILE >> 4;
+    constexpr uint32_t A16 = (uint32_t)A_BOX >> 4, B16 = (uint32_t)SS_PLANE >> 4;
 #pragma unroll
     for (int kc = 0; kc < 2; ++kc) {
         const int k = q + 2 * kc;
@@ -586,7 +591,7 @@ __device__ __forceinline__ void issue_stage_ss(uint32_t tmem, uint64_t a_stage, 
             for (int i = 0; i < 3; ++i) {
                 const int j = k - i;
                 if (j < 0 || j >= NDB) continue;
-                // K slice kk = bytes [32kk, 32kk+32) of each 64-byte row: +2 in 16-byte units
+                // K slice kk = bytes [32kk, 32kk+32) of the stage's 64 bytes of each row: +2 in 16-byte units
                 umma_ss_i8(acc, a_stage + (uint64_t)(i * A16 + kk * 2), b_stage + (uint64_t)(j * B16 + kk * 2), idesc,
                            (first && fresh) ? 0u : 1u);
                 first = false;
@@ -602,12 +607,13 @@ __global__ void __launch_bounds__(SS_NTHREADS, 1)
     static_assert(PT == 16, "former pixels per thread");
     static_assert(NACC * BN <= TMEM_COLS, "accumulators must fit in TMEM");
     static_assert(NEPI == SS_NWARP_B, "the formers run the epilogue");
+    static_assert(SS_NAS <= SS_NSB, "the D2 ring waits on B-stage releases");
 
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char *smem = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     unsigned char *bin = smem;                               // SS_NBI × SS_HALF_BYTES
-    unsigned char *bdig = bin + SS_NBI * SS_HALF_BYTES;      // SS_NSB × SS_STAGE_BD
-    unsigned char *atile = bdig + SS_NSB * SS_STAGE_BD;      // SS_NAS × 3 × A_BOX
+    unsigned char *bdig = bin + SS_NBI * SS_HALF_BYTES;      // 2 × SS_SLOT
+    unsigned char *atile = bdig + 2 * SS_SLOT;               // SS_NAS × 3 × A_BOX
     float *d1rows = reinterpret_cast<float *>(atile + SS_NAS * 3 * A_BOX);  // SS_NBI × SS_HALF fp32
     uint64_t *bars = reinterpret_cast<uint64_t *>(d1rows + SS_NBI * SS_HALF);
     uint64_t *as_full = bars, *as_empty = as_full + SS_NAS;
@@ -680,7 +686,10 @@ __global__ void __launch_bounds__(SS_NTHREADS, 1)
                 const int nb = stages_of(v);
                 for (int it = 0; it < nb; ++it, ++gs) {
                     const int s = gs % SS_NAS;
-                    if (!mbar_wait(&as_empty[s], ((gs / SS_NAS) & 1) ^ 1, abort_flag, err, 18)) { ok = false; break; }
+                    // the tile slot's previous stage (gs − SS_NAS) has retired when its B stage is released:
+                    // one commit per stage serves both rings
+                    if (gs >= SS_NAS && !mbar_wait(&st_empty[(gs - SS_NAS) % SS_NSB], ((gs - SS_NAS) / SS_NSB) & 1,
+                                                   abort_flag, err, 18)) { ok = false; break; }
                     unsigned char *t = atile + s * 3 * A_BOX;
                     mbar_expect_tx(&as_full[s], 3 * A_BOX);
                     const int x = (int)(v.x_begin + (long)it * SS_KB);
@@ -702,7 +711,7 @@ __global__ void __launch_bounds__(SS_NTHREADS, 1)
                                    ((uint32_t)(BM >> 4) << 24);
             // descriptors are linear in the start address (bits 0-13, 16-byte units)
             const uint64_t adesc0 = smem_desc_sw64(smem_u32(atile));
-            const uint64_t bdesc0 = smem_desc_sw64(smem_u32(bdig));
+            const uint64_t bdesc0 = smem_desc_sw128(smem_u32(bdig));
             int gs = 0, seq = 0;
             for (int g = blockIdx.x; g < nitems && ok; g += gridDim.x, ++seq) {
                 const int nb = stages_of(decode<BN>(jobs, items, g));
@@ -713,9 +722,9 @@ __global__ void __launch_bounds__(SS_NTHREADS, 1)
                     if (!mbar_wait(&as_full[sa], ((gs / SS_NAS) & 1), abort_flag, err, 19)) { ok = false; break; }
                     fence_after();
                     issue_stage_ss(tmem, adesc0 + (uint64_t)((sa * 3 * A_BOX) >> 4),
-                                   bdesc0 + (uint64_t)((s * SS_STAGE_BD) >> 4), idesc, q, it == 0);
+                                   bdesc0 + (uint64_t)((((gs >> 1) & 1) * SS_SLOT + (gs & 1) * 64) >> 4), idesc, q,
+                                   it == 0);
                     umma_commit(&st_empty[s]);
-                    umma_commit(&as_empty[sa]);
                 }
                 if (ok) umma_commit(acc_full);
             }
@@ -732,8 +741,8 @@ __global__ void __launch_bounds__(SS_NTHREADS, 1)
         const int n = tid % BN, sg = tid / BN;
         const int half = sg >> 1;
         const int c0 = (sg & 1) * 4;  // first 16-byte chunk of the thread's 16 pixels in the half's 128-byte row
-        // destination: 16-byte chunk sg of each 64-byte digit row, at its 64B-swizzled position
-        const int dst_off = n * SS_KB + ((sg ^ ((n >> 1) & 3)) << 4);
+        // destination: 16-byte chunk 4(gs & 1) + sg of the 128-byte digit row n, at its 128B-swizzled
+        // position (the chunk index is XORed with the row's low three bits)
         int gs = 0, seq = 0;
         for (int g = blockIdx.x; g < nitems && ok; g += gridDim.x, ++seq) {
             const ItemView v = decode<BN>(jobs, items, g);
@@ -765,10 +774,10 @@ __global__ void __launch_bounds__(SS_NTHREADS, 1)
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&bin_empty[si]);
                 if (!mbar_wait_warp(&st_empty[s], ((gs / SS_NSB) & 1) ^ 1, abort_flag, err, 17)) { ok = false; break; }
-                unsigned char *dst = bdig + s * SS_STAGE_BD + dst_off;
+                unsigned char *dst = bdig + ((gs >> 1) & 1) * SS_SLOT + n * 128 + (((4 * (gs & 1) + sg) ^ (n & 7)) << 4);
 #pragma unroll
                 for (int d = 0; d < NDB; ++d)
-                    *reinterpret_cast<uint4 *>(dst + d * SS_TILE) = make_uint4(w[d][0], w[d][1], w[d][2], w[d][3]);
+                    *reinterpret_cast<uint4 *>(dst + d * SS_PLANE) = make_uint4(w[d][0], w[d][1], w[d][2], w[d][3]);
                 fence_proxy_async_smem();
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&st_full[s]);
@@ -832,7 +841,7 @@ __global__ void __launch_bounds__(SS_NTHREADS, 1)
 
 size_t smem_bytes_ss()
 {
-    return 1024 + (size_t)SS_NBI * SS_HALF_BYTES + (size_t)SS_NSB * SS_STAGE_BD + (size_t)SS_NAS * 3 * A_BOX +
+    return 1024 + (size_t)SS_NBI * SS_HALF_BYTES + 2 * (size_t)SS_SLOT + (size_t)SS_NAS * 3 * A_BOX +
            (size_t)SS_NBI * SS_HALF * 4 + 256;
 }
 
