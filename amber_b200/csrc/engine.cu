@@ -236,10 +236,11 @@ void Engine::finish(Request *r)
         }
     }
     r->counts = s->counts;
-    info.products += s->last_products;
+    const double products = s->last_products;
     amber_cuda_destroy(s);
     r->sub = nullptr;
     std::lock_guard<std::mutex> lk(mu);
+    info.products += products;
     in_use -= r->footprint;
     r->state = Request::DONE;
     r->t_done = now_ms();
@@ -284,6 +285,9 @@ void Engine::loop()
             round = active;
         }
         const double t0 = now_ms();
+        // this round's share of the statistics, published under the lock at its end
+        double setup_ms = 0, maps_ms = 0, contract_ms = 0, finish_ms = 0;
+        long launches = 0;
         owner->phase_used = 0;  // per-phase timing events are reused round after round
         // one map-set batch of every active request
         std::vector<I8Job> jobs;
@@ -292,7 +296,7 @@ void Engine::loop()
             int rc = AMBER_OK;
             double ta = now_ms();
             if (!r->started) rc = setup(r);
-            info.setup_ms += now_ms() - ta;
+            setup_ms += now_ms() - ta;
             if (!rc && run_finished(r->run)) {
                 finish(r);  // no triangles at all
                 continue;
@@ -301,7 +305,7 @@ void Engine::loop()
                 ta = now_ms();
                 rc = run_next_batch(r->sub, r->run, &jobs);
                 rc = rc < 0 ? rc : AMBER_OK;
-                info.maps_ms += now_ms() - ta;
+                maps_ms += now_ms() - ta;
             }
             if (rc) {
                 fail_req(r, rc, r->sub ? r->sub->err : std::string("context creation failed"));
@@ -314,9 +318,9 @@ void Engine::loop()
         if (!jobs.empty()) {
             const long before = owner->contractions;
             rc = contract_i8_jobs(owner, jobs);
-            info.contraction_launches += owner->contractions - before;
+            launches = owner->contractions - before;
         }
-        info.contract_ms += now_ms() - tc;
+        contract_ms = now_ms() - tc;
         tc = now_ms();
         if (rc) {
             const std::string msg = owner->err;
@@ -325,7 +329,13 @@ void Engine::loop()
             for (Request *r : in_round)
                 if (run_finished(r->run)) finish(r);
         }
-        info.finish_ms += now_ms() - tc;
+        finish_ms = now_ms() - tc;
+        std::lock_guard<std::mutex> lk(mu);
+        info.setup_ms += setup_ms;
+        info.maps_ms += maps_ms;
+        info.contract_ms += contract_ms;
+        info.finish_ms += finish_ms;
+        info.contraction_launches += launches;
         info.rounds += 1;
         info.busy_ms += now_ms() - t0;
     }
