@@ -116,6 +116,34 @@ def test_mixed_vs_fp64_full_size(lib_built):
     assert ei.max() <= TOL["mixed"], (sample[int(ei.argmax())], ei.max())
 
 
+def test_isosceles_symmetry_full_size(lib_built):
+    """A size-independent property at full size: for a triangle with r2 = r3 the two outer maps are
+    the same, so T_p1[p2, p3] is symmetric and so are the lag arrays, bldnu[Δ2, Δ3] = bldnu[Δ3, Δ2]
+    (and the mask sums).  The plain FP64 path keeps it to rounding; the mixed path forms the two
+    operands differently (plain digits and product digits), so there it holds to twice its error
+    bound.  Counts are symmetric exactly."""
+    import amber_b200
+    real = synth.config2(seed=1)
+    out = {}
+    for prec in ("mixed", "fp64", "fp64_abs"):
+        with amber_b200.Estimator(precision=prec) as est:
+            est.load_grid(real.gv, real.counts, real.du, real.flag_key)
+            est.set_rings(real.ulow, real.uhigh)
+            est.set_channels(real.nc10, real.uf_chans)
+            tri = est.calcr()[:, :3].astype(np.int32)
+            iso = tri[(tri[:, 1] == tri[:, 2]) & (tri[:, 0] != tri[:, 1])]
+            sample = iso[-3:]  # the largest maps with r2 = r3 < r1
+            est.run(sample, want_v2=True)
+            out[prec] = est.fetch(want_v2=True)
+    (ab, _, at) = out["fp64_abs"]
+    for prec, tol in (("fp64", 1e-10), ("mixed", 2 * TOL["mixed"])):
+        bl, nd, nt = out[prec]
+        for i in range(len(bl)):
+            np.testing.assert_array_equal(nd[i], nd[i].T)
+            assert (np.abs(bl[i] - bl[i].T) <= tol * ab[i] + 1e-300).all(), prec
+            assert (np.abs(nt[i] - nt[i].T) <= tol * at[i] + 1e-300).all(), prec
+
+
 def test_split_anchor_groups_match(lib_built):
     """A job whose partial tiles exceed the per-launch cap runs as anchor groups whose lag sums add
     up in order.  128-pixel chunks on the Ng1 = 354 triangle of the single-realisation workload
