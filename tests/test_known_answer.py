@@ -105,3 +105,26 @@ def test_gridding_known_answer_on_the_device():
         gv, nt = est.grid_vis(32, 2, 0.5, 6.0, nu0, 1, randpar, data)
     g_o, n_o = oracle.grid_vis(32, 2, 0.5, 6.0, nu0, 1, randpar, data)
     assert np.array_equal(gv, g_o) and np.array_equal(nt, n_o) and nt.sum() == 7
+
+
+def test_oracle_lag_symmetries():
+    """Properties of the lag arrays that follow from the estimator's definition: with r2 = r3,
+    bldnu[Δ2, Δ3] = bldnu[Δ3, Δ2]; with r1 = r2, swapping the roles of p1 and p2 gives
+    bldnu[Δ2, Δ3] = bldnu[−Δ2, Δ3 − Δ2] (flags included: the channel weights are symmetric)."""
+    real = synth.tiny(40, 10, seed=71, nbins=4, hi=18.0, nc10=4, flagged=[2, 7])
+    _, res = oracle.estimate(real, version=1, with_absscale=True)
+    n10 = real.nc10
+    seen = set()
+    for r in res:
+        B, A = r["bldnu"], r["absscale"] + 1e-300
+        if r["r2"] == r["r3"]:
+            assert (np.abs(B - B.T) <= 1e-12 * A).all()
+            seen.add("23")
+        if r["r1"] == r["r2"]:
+            for d2 in range(-n10, n10 + 1):
+                for d3 in range(max(-n10, d2 - n10), min(n10, d2 + n10) + 1):
+                    a, b = B[d2 + n10, d3 + n10], B[-d2 + n10, d3 - d2 + n10]
+                    assert abs(a - b) <= 1e-12 * A[d2 + n10, d3 + n10]
+            seen.add("12")
+        np.testing.assert_array_equal(r["numdnu"], r["numdnu"].T)
+    assert seen == {"12", "23"}
