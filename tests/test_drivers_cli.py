@@ -59,3 +59,15 @@ def test_cylbs_parameter_checks():
     p = amber_b200.cylbs_params(window=True, denominator="mask", n_cut=3)
     assert (p.n_cut, p.window, p.denominator) == (3, 1, 1)
     assert p.mabs_norm == amber_b200.reference_cylbs_constants()["mabs_norm"]
+
+
+def test_grid_vis_rejects_bad_record_shapes():
+    """The Python wrapper checks the record arrays before any library call (no GPU needed)."""
+    est = amber_b200.Estimator.__new__(amber_b200.Estimator)  # no context: the checks come first
+    randpar = np.zeros((5, 3), dtype=np.float32)
+    for bad in (np.zeros((5, 3, 2), np.float32),        # not [G, nchan, nstokes, 3]
+                np.zeros((5, 2, 1, 3), np.float32),     # fewer channels than nc
+                np.zeros((4, 3, 1, 3), np.float32),     # record count differs from randpar
+                np.zeros((5, 3, 1, 2), np.float32)):    # not (re, im, wt)
+        with pytest.raises(ValueError):
+            est.grid_vis(16, 3, 0.5, 4.0, 1.5e8, 1, randpar, bad)
