@@ -463,6 +463,14 @@ int amber_cuda_result(amber_cuda_ctx *c, int64_t ticket, int max_tri, double *rd
         std::lock_guard<std::mutex> lk(e->mu);
         auto it = e->reqs.find(ticket);
         if (it == e->reqs.end()) return AMBER_ERR_ARG;
+        if (it->second->state == Request::FAILED) {
+            // a failed request is forgotten here too, with its copied inputs: nothing else
+            // frees them before the context is destroyed
+            const int rc = it->second->rc ? it->second->rc : AMBER_ERR_STATE;
+            c->err = "request " + std::to_string(ticket) + ": " + it->second->err;
+            e->reqs.erase(it);
+            return rc;
+        }
         if (it->second->state != Request::DONE) return AMBER_ERR_STATE;
         const int ntri = (int)it->second->tri.size() / 3;
         if (ntri > max_tri) return amber::fail(c, AMBER_ERR_ARG, "result: %d triangles, room for %d", ntri, max_tri);

@@ -23,6 +23,8 @@
 #include <algorithm>
 #include <mutex>
 
+#include <cuda.h>
+
 #include "common.cuh"
 
 namespace {
@@ -128,9 +130,12 @@ __global__ void noalloc_batch_sum(const double *__restrict__ partial, long nunit
     lag[d] = accumulate ? lag[d] + s : s;
 }
 
-// Device address of the scratch array, looked up once per device.
+// Device address of the scratch array, looked up once per device and context: a context
+// destroyed and recreated (cudaDeviceReset) maps the array anew, so the cached address is
+// kept together with the context it belongs to and looked up again when that changes.
 std::mutex g_mutex;
 double *g_scratch_ptr[64] = {};
+CUcontext g_scratch_ctx[64] = {};
 
 }  // namespace
 
@@ -151,12 +156,32 @@ extern "C" int amber_cuda_contract_fp64_noalloc(const double *d_m1, const double
     if (ncsize > kPartialDoubles)
         return reject(AMBER_ERR_ARG, "lag window too large for the 8 MiB scratch (nclen^2 must be <= 1044480, nc10 <= 510)");
 
+    cudaStream_t s = (cudaStream_t)stream;
+    // The channel tables below are copied from a host buffer that lives only for this call.
+    // A stream under capture would record that copy for later replays instead of making it
+    // now, so a capturing stream is refused.
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cap) != cudaSuccess) {
+        cudaGetLastError();
+        return reject(AMBER_ERR_ARG, "invalid stream");
+    }
+    if (cap != cudaStreamCaptureStatusNone)
+        return reject(AMBER_ERR_ARG, "stream is being captured: this call uploads host channel tables when it is made");
+
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return reject(AMBER_ERR_NODEV, "no device");
     double *scratch;
     {
         std::lock_guard<std::mutex> lock(g_mutex);
-        if (!g_scratch_ptr[dev]) {
+        // cudaGetDevice does not initialise the device's primary context; cudaSetDevice does
+        // and makes it current, so that the context handle below exists
+        if (cudaSetDevice(dev) != cudaSuccess) {
+            cudaGetLastError();
+            return reject(AMBER_ERR_NODEV, "cannot make the device current");
+        }
+        CUcontext ctx = nullptr;
+        if (cuCtxGetCurrent(&ctx) != CUDA_SUCCESS || !ctx) return reject(AMBER_ERR_CUDA, "no current context");
+        if (!g_scratch_ptr[dev] || g_scratch_ctx[dev] != ctx) {
             void *p = nullptr;
             cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
             if (e != cudaSuccess || !p) {
@@ -164,6 +189,7 @@ extern "C" int amber_cuda_contract_fp64_noalloc(const double *d_m1, const double
                 return reject(AMBER_ERR_CUDA, "cudaGetSymbolAddress of the scratch array failed");
             }
             g_scratch_ptr[dev] = (double *)p;
+            g_scratch_ctx[dev] = ctx;
         }
         scratch = g_scratch_ptr[dev];
     }
@@ -176,7 +202,6 @@ extern "C" int amber_cuda_contract_fp64_noalloc(const double *d_m1, const double
         table[p] = weight[p];
         if (weight[p] > 0) table[nc + na++] = (int)p;
     }
-    cudaStream_t s = (cudaStream_t)stream;
     int *d_table = reinterpret_cast<int *>(scratch + kPartialDoubles);
     if (cudaMemcpyAsync(d_table, table, sizeof(int) * (nc + (na > 0 ? na : 1)), cudaMemcpyHostToDevice, s) !=
         cudaSuccess) {

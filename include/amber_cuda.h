@@ -234,7 +234,9 @@ AMBER_API int amber_cuda_grid_vis_collapsed(amber_cuda_ctx *ctx, long NN, long n
  * AMBER_ERR_TIMEOUT when the limit passes first, the request keeps running)
  * and gives its triangle count; a failed request returns its error.
  * amber_cuda_result then copies the outputs into caller buffers and forgets
- * the request: rdata [ntri][4] as amber_cuda_calcr, bldnu and numtri (v2)
+ * the request (for a failed request it returns the request's error and frees
+ * what the request holds; until then a failed request keeps its copied
+ * inputs): rdata [ntri][4] as amber_cuda_calcr, bldnu and numtri (v2)
  * [ntri][nclen²] FP64, numdnu [ntri][nclen²] int64, the request's latency in
  * ms from enqueue to completion and, when the request gave cylbs, the
  * cylindrical bispectra [ntri][N][N] (N = 2·(nc10 + 1 − n_cut) − 1) as
@@ -296,9 +298,12 @@ AMBER_API int amber_cuda_engine_stats(amber_cuda_ctx *ctx, amber_cuda_engine_inf
  * exits; nc ≤ 4096 and nclen² ≤ 1044480 (nc10 ≤ 510); larger sizes are
  * rejected with AMBER_ERR_ARG.  The first call on a device looks up the
  * array's device address (cudaGetSymbolAddress, with that device current), so
- * make that first call before any stream capture.  Every call shares the
- * array: calls that overlap on the GPU (different streams, or host threads)
- * race.  Work is enqueued on `stream` (a cudaStream_t, NULL for the default
+ * make that first call before any stream capture; the address is looked up
+ * again when the device's context has changed (after a cudaDeviceReset).
+ * Each call uploads its channel tables from host memory when it is made, so a
+ * stream that is being captured is refused with AMBER_ERR_ARG.  Every call
+ * shares the array: calls that overlap on the GPU (different streams, or host
+ * threads) race.  Work is enqueued on `stream` (a cudaStream_t, NULL for the default
  * stream); the caller synchronises.  err_msg (may be NULL) receives a
  * message on failure. */
 AMBER_API int amber_cuda_contract_fp64_noalloc(const double *m1, const double *m2, const double *m3, long nc,

@@ -24,6 +24,9 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
+# Where the reference's own sources are read from (to build _ref/ and to import its Python
+# readers in tests); override with AMBER_REF_DIR.  Absent on machines that only run the built files.
+REFERENCE_SOURCES = os.environ.get("AMBER_REF_DIR", "/root/reference")
 _lib = None
 
 _dp = ctypes.POINTER(ctypes.c_double)

@@ -110,7 +110,7 @@ def cylbs_case(nc10=30, seed=11):
     import types
     sys.modules.setdefault("matplotlib", types.ModuleType("matplotlib"))
     sys.modules.setdefault("matplotlib.pyplot", types.ModuleType("matplotlib.pyplot"))
-    sys.path.insert(0, "/root/reference")
+    sys.path.insert(0, oracle.REFERENCE_SOURCES)
     mf = importlib.import_module("mabs_funcs")
     nclen = 2 * nc10 + 1
     mf.nc10, mf.nclen, mf.ncsize = nc10, nclen, nclen * nclen

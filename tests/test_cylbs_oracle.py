@@ -49,7 +49,7 @@ def test_reference_constants_match_library_defaults():
     assert c["dnu_mhz"] == float(g["dnu"])
 
 
-REF = "/root/reference"
+from oracle import REFERENCE_SOURCES as REF  # noqa: E402
 
 
 @pytest.mark.skipif(not os.path.exists(os.path.join(REF, "mabs_funcs.py")), reason="reference sources not present")

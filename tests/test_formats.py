@@ -8,8 +8,7 @@ import numpy as np
 import pytest
 
 from amber_b200 import formats, synth
-
-REF = "/root/reference"
+from oracle import REFERENCE_SOURCES as REF
 
 
 def test_gv_roundtrip(tmp_path):
