@@ -179,8 +179,17 @@ extern "C" int amber_cuda_contract_fp64_noalloc(const double *d_m1, const double
             cudaGetLastError();
             return reject(AMBER_ERR_NODEV, "cannot make the device current");
         }
+        // the driver call is resolved through the runtime, so the library needs no link-time libcuda
+        static CUresult (*ctx_current)(CUcontext *) = nullptr;
+        if (!ctx_current) {
+            void *fn = nullptr;
+            cudaDriverEntryPointQueryResult q;
+            if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &q) != cudaSuccess || !fn)
+                return reject(AMBER_ERR_CUDA, "cuCtxGetCurrent unavailable");
+            ctx_current = (CUresult(*)(CUcontext *))fn;
+        }
         CUcontext ctx = nullptr;
-        if (cuCtxGetCurrent(&ctx) != CUDA_SUCCESS || !ctx) return reject(AMBER_ERR_CUDA, "no current context");
+        if (ctx_current(&ctx) != CUDA_SUCCESS || !ctx) return reject(AMBER_ERR_CUDA, "no current context");
         if (!g_scratch_ptr[dev] || g_scratch_ctx[dev] != ctx) {
             void *p = nullptr;
             cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
