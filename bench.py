@@ -373,6 +373,28 @@ def stages_section(amber_b200, synth, dev, reps=5):
     return res
 
 
+def gridding_section(amber_b200, synth, dev, reps=5):
+    """Gridding alone (amber_cuda_grid_vis, 3_vcg's group_loop_gridding): 100k visibility records x 128
+    channels x 2 Stokes onto the 256^2 grid, flag_key 1.  Reports the median wall time of the
+    synchronous call (records up, grid down) and the algorithmic bytes of the device work: the
+    RR payload read once (12 B per record-channel) plus u, v (8 B per record), and the grid written
+    once (24 B per cell-channel: re, im, count)."""
+    nn, du, nc, nrec = 256, 0.5, 128, 100000
+    randpar, data = synth.make_visibilities(nn, du, nc, nrec, 91)
+    umax = 0.95 * du * nn / 2
+    ts = []
+    with amber_b200.Estimator(device=dev, precision="fp64") as est:
+        for _ in range(reps + 1):
+            t0 = time.perf_counter()
+            est.grid_vis(nn, nc, du, umax, np.float32(synth.NU0), 1, randpar, data)
+            ts.append(time.perf_counter() - t0)
+    h = nn // 2 + 1
+    return {"workload": f"gridding: {nrec} records x {nc} channels x 2 Stokes onto the {nn}^2 grid (flag_key 1)",
+            "grid_call_ms_median": 1e3 * float(np.median(ts[1:])),
+            "algorithmic_bytes": int(nrec * (8 + 12 * nc) + nn * h * nc * 24),
+            "record_bytes_copied_in": int(randpar.nbytes + data.nbytes)}
+
+
 def maps_section(amber_b200, synth, dev):
     """The MAPS two-point function (amber_cuda_cl_dnu; maps.c's 15 bins from 1 to 500) of the
     single-realisation grid, against the reference's own cl_dnu pair loop (oracle/_ref/ref_maps,
@@ -426,6 +448,8 @@ def main():
                     help="time the stages beside the contraction (cylindrical bispectra, gridding with collapse)")
     ap.add_argument("--maps", action="store_true",
                     help="measure the MAPS two-point function (amber_cuda_cl_dnu) instead of the default step")
+    ap.add_argument("--gridding", action="store_true",
+                    help="time the gridding stage alone (100k records x 128 channels onto 256^2)")
     ap.add_argument("--config4", action="store_true",
                     help="measure a fixed sample of the large cube (512^2, 384 channels) instead of the default step")
     args = ap.parse_args()
@@ -466,6 +490,13 @@ def main():
             st = stages_section(amber_b200, synth, local)
             print(json.dumps(dict(impl="amber_b200", n_gpus=1, data="synthetic", config={"workload": st["workload"]},
                                   **{k: v for k, v in st.items() if k != "workload"})))
+        return 0
+
+    if args.gridding:
+        if rank == 0:
+            gr = gridding_section(amber_b200, synth, local)
+            print(json.dumps(dict(impl="amber_b200", n_gpus=1, dtype="f64 sums of f32 records", data="synthetic",
+                                  config={"workload": gr["workload"]}, **{k: v for k, v in gr.items() if k != "workload"})))
         return 0
 
     if args.maps:
