@@ -18,7 +18,7 @@ LIB = os.path.join(HERE, "libamber_cuda.so")
 DRIVER = os.path.join(HERE, "amber_gpu")
 VCG_DRIVER = os.path.join(HERE, "vcg_gpu")
 MAPS_DRIVER = os.path.join(HERE, "maps_gpu")
-SOURCES = ["api.cu", "maps.cu", "contract64.cu", "contract_tc.cu", "contract_i8.cu", "grid.cu", "noalloc.cu", "engine.cu", "cylbs.cu", "cldnu.cu"]
+SOURCES = ["api.cu", "maps.cu", "lagspace.cu", "contract64.cu", "contract_tc.cu", "contract_i8.cu", "grid.cu", "noalloc.cu", "engine.cu", "cylbs.cu", "cldnu.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -12,7 +12,7 @@
 #include <set>
 #include <vector>
 
-#include "common.cuh"
+#include "lagspace.cuh"
 
 namespace amber {
 
@@ -251,9 +251,9 @@ int run_begin(amber_cuda_ctx *c, RunState &st, int ntri, const int *tri, int wan
 size_t map_slot_bytes(int precision, long ng, long nc, int want_v2)
 {
     const size_t vbytes = precision == AMBER_PREC_FP64 ? 8 : (precision == AMBER_PREC_MIXED ? 7 : 4);
-    const long kalign = precision == AMBER_PREC_MIXED ? 128 : 64;
+    const long kalign = precision == AMBER_PREC_MIXED ? LS_BLOCK : 64;
     const long k = ng * ng, kp = (k + kalign - 1) / kalign * kalign;
-    const size_t per_pass = vbytes * (size_t)nc * kp + 8 * (size_t)nc;
+    const size_t per_pass = vbytes * (size_t)nc * kp + 8 * (size_t)nc + 4 * (size_t)(kp / LS_BLOCK + 1);
     // + the map builder's column-pass intermediate (double2 per ring row, column and channel)
     const size_t y = sizeof(double2) * (size_t)ng * (size_t)(ng / 3 + 1) * (size_t)nc;
     return per_pass * (want_v2 ? 2 : 1) + y;
@@ -275,9 +275,10 @@ int run_next_batch(amber_cuda_ctx *c, RunState &st, std::vector<I8Job> *jobs)
     const long ncsize = (long)nclen * nclen;
     double *res = (double *)c->results.p;
     const size_t vbytes = prec == AMBER_PREC_FP64 ? 8 : (prec == AMBER_PREC_MIXED ? 7 : 4);
-    const long kalign = prec == AMBER_PREC_MIXED ? 128 : 64;
+    const long kalign = prec == AMBER_PREC_MIXED ? LS_BLOCK : 64;
     const long k = g.ng * g.ng, kp = (k + kalign - 1) / kalign * kalign;
-    const size_t per_slot = vbytes * (size_t)c->nc * kp + 8 * (size_t)c->nc;
+    const long nblk = kp / LS_BLOCK;
+    const size_t per_slot = vbytes * (size_t)c->nc * kp + 8 * (size_t)c->nc + 4 * (size_t)(nblk + 1);
     // The next batch of the group: triangles whose ring union fits the budget.
     size_t spare = c->budget > c->held ? c->budget - c->held : 0;
     spare += c->maps_d.bytes + c->maps_i.bytes + c->y.bytes;
@@ -323,22 +324,19 @@ int run_next_batch(amber_cuda_ctx *c, RunState &st, std::vector<I8Job> *jobs)
             job.out_lo = (uint16_t *)p + nvals;
         } else {
             job.out_f32 = (float *)p;
-            job.d0 = (int8_t *)(p + 4 * nvals);
-            job.d1 = job.d0 + nvals;
-            job.d2 = job.d1 + nvals;
-            job.expo = (int *)(p + 7 * nvals);
-            job.rowmax = (unsigned *)(job.expo + nrows);
+            job.weight = (const int *)c->d_weight.p;
+            job.dig = (int8_t *)(p + 4 * nvals);
+            job.bexp = (int *)(p + 7 * nvals);
             if (dm_base) {
                 dm_base->f32 = job.out_f32;
-                dm_base->d0 = job.d0;
-                dm_base->d1 = job.d1;
-                dm_base->d2 = job.d2;
-                dm_base->expo = job.expo;
+                dm_base->dig = job.dig;
+                dm_base->bexp = job.bexp;
             }
         }
     };
     std::vector<I8Job> local;
     std::vector<I8Job> *jl = jobs ? jobs : &local;
+    std::vector<F64Job> f64jobs;
     DigitMaps dmaps[2];
     for (int pass = 0; pass < (want_v2 ? 2 : 1); ++pass) {
         MapJob job{};
@@ -356,10 +354,6 @@ int run_next_batch(amber_cuda_ctx *c, RunState &st, std::vector<I8Job> *jobs)
             job.hi.push_back(c->uhigh[r]);
         }
         carve(pass == 0 ? c->maps_d.p : c->maps_i.p, job, &dmaps[pass]);
-        if (job.rowmax &&
-            (rc = cuda_check(c, cudaMemsetAsync(job.rowmax, 0, sizeof(unsigned) * nrows, c->stream),
-                             "row max reset")))
-            return rc;
         phase_begin(c, 0);
         rc = build_maps(c, job);
         phase_end(c);
@@ -377,19 +371,17 @@ int run_next_batch(amber_cuda_ctx *c, RunState &st, std::vector<I8Job> *jobs)
                 auto slot = [&](size_t s) {
                     DigitMaps d;
                     d.f32 = b.f32 + s * ss;
-                    d.d0 = b.d0 + s * ss;
-                    d.d1 = b.d1 + s * ss;
-                    d.d2 = b.d2 + s * ss;
-                    d.expo = b.expo + s * c->nc;
+                    d.dig = b.dig + s * 3 * ss;
+                    d.bexp = b.bexp + s * nblk;
                     return d;
                 };
                 I8Job jb;
                 jb.m1 = slot(s1); jb.m2 = slot(s2); jb.m3 = slot(s3);
                 jb.k = k; jb.kp = kp;
                 jb.nc = (int)c->nc; jb.nc10 = c->nc10;
-                jb.anchors = (const int *)c->d_anchors.p;
-                jb.weight = (const int *)c->d_weight.p;
+                jb.weight = &c->weight;
                 jb.nanchors = (int)c->anchors.size();
+                jb.mask_pass = pass == 1;
                 jb.lag_out = lag;
                 jl->push_back(jb);
                 rc = AMBER_OK;
@@ -400,13 +392,14 @@ int run_next_batch(amber_cuda_ctx *c, RunState &st, std::vector<I8Job> *jobs)
                                      lo + s3 * ss, k, kp, lag);
             } else {
                 const double *m = (const double *)base;
-                rc = contract_fp64(c, m + s1 * ss, m + s2 * ss, m + s3 * ss, k, kp, lag);
+                f64jobs.push_back(F64Job{m + s1 * ss, m + s2 * ss, m + s3 * ss, k, kp, lag});
             }
             if (rc) return rc;
         }
         c->last_products += (double)c->total_vcp * (double)k * (want_v2 ? 2.0 : 1.0);
     }
     if (!local.empty() && (rc = contract_i8_jobs(c, local))) return rc;
+    if (!f64jobs.empty() && (rc = contract_fp64_jobs(c, f64jobs))) return rc;
     return 1;
 }
 
@@ -477,7 +470,7 @@ void amber_cuda_destroy(amber_cuda_ctx *c)
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);
     DevBuf *bufs[] = {&c->grid, &c->mask, &c->d_weight, &c->d_anchors, &c->y, &c->maps_d, &c->maps_i,
-                      &c->partial, &c->results, &c->ring_lohi, &c->misc, &c->mixed_scratch, &c->lagred, &c->jobdesc, &c->lagtrial};
+                      &c->partial, &c->results, &c->ring_lohi, &c->misc, &c->mixed_scratch, &c->lagred, &c->jobdesc, &c->lagtrial, &c->lsred};
     for (DevBuf *b : bufs) release(c, *b);
     if (c->stage) cudaFreeHost(c->stage);
     c->stage = nullptr;

@@ -83,6 +83,7 @@ struct amber_cuda_ctx {
     amber::DevBuf lagred;  // two-pass lag reduction: per-group sums and compensations
     amber::DevBuf jobdesc; // contraction job descriptors and work items
     amber::DevBuf lagtrial; // autotuner: lag array of a discarded trial run
+    amber::DevBuf lsred;    // lag-space reduction: job descriptors
     void *stage = nullptr; // pinned host staging of the job descriptors
     size_t stage_bytes = 0;
     amber::Engine *engine = nullptr;  // batched requests, created on the first enqueue
@@ -135,36 +136,44 @@ struct MapJob {
     std::vector<double> lo, hi;  // host copies
     double *out_f64;
     uint16_t *out_hi, *out_lo;  // bf16 planes
-    float *out_f32;
-    unsigned *rowmax;             // per (slot, channel) max |fp32 value| (zeroed by the caller)
-    int8_t *d0, *d1, *d2;         // int8 digit planes (written from out_f32 when non-null)
-    int *expo;                    // per (slot, channel) row exponent of the digits
+    float *out_f32;               // mixed path: maps weighted by the channel multiplicities
+    const int *weight;            // device multiplicities of the source channels (mixed path)
+    int8_t *dig;                  // mixed path: digit planes [slot][3][kp/16][nch][16] (kp multiple of 256)
+    int *bexp;                    // mixed path: exponent per (slot, 256-pixel block)
 };
 int build_maps(amber_cuda_ctx *c, const MapJob &job);
 
 // FP64 contraction of one triangle into a lag array (device).
 int contract_fp64(amber_cuda_ctx *c, const double *m1, const double *m2, const double *m3, long k, long kp,
                   double *lag_out);
+// One FP64 contraction job (one triangle's D or mask pass on the context's channels).
+struct F64Job {
+    const double *m1, *m2, *m3;  // [nc][kp] maps of r1, r2, r3
+    long k, kp;
+    double *lag_out;             // device FP64 lag array [nclen²]
+};
+// All jobs in as few launches as the partial-tile memory allows, then one reduction per launch.
+int contract_fp64_jobs(amber_cuda_ctx *c, const std::vector<F64Job> &jobs);
 // Split-BF16×3 contraction (tcgen05, FP32 accumulation in TMEM).
 int contract_bf16x3(amber_cuda_ctx *c, const uint16_t *h1, const uint16_t *l1, const uint16_t *h2,
                     const uint16_t *l2, const uint16_t *h3, const uint16_t *l3, long k, long kp, double *lag_out);
 // Mixed-precision contraction: base-254 int8 digits on the tensor cores
 // (tcgen05 kind::i8, exact int32 accumulation in TMEM).
 struct DigitMaps {
-    const float *f32;                 // [nc][kp]
-    const int8_t *d0, *d1, *d2;       // [nc][kp]
-    const int *expo;                  // [nc]
+    const float *f32;                 // [nc][kp], weighted by the channel multiplicities
+    const int8_t *dig;                // [3][kp/16][nc][16] base-254 digits of f32
+    const int *bexp;                  // [kp/256] block exponents
 };
 int contract_i8(amber_cuda_ctx *c, const DigitMaps &m1, const DigitMaps &m2, const DigitMaps &m3, long k, long kp,
                 double *lag_out);
 // One mixed-precision contraction job: one triangle's D or mask pass of one realisation.
 struct I8Job {
     DigitMaps m1, m2, m3;   // ring maps of r1, r2, r3 on the job's Ng1 grid
-    long k, kp;             // pixels, row stride
+    long k, kp;             // pixels, row stride (a multiple of 256)
     int nc, nc10;           // the realisation's channel count and lag half-width
-    const int *anchors;     // device: channels with weight > 0
-    const int *weight;      // device: channel multiplicities
+    const std::vector<int> *weight;  // host: channel multiplicities (the planner's anchor groups)
     int nanchors;
+    bool mask_pass;         // sampling-mask maps: four product digits (a second sweep for class 3)
     double *lag_out;        // device: FP64 lag array [nclen²]
 };
 // All jobs in as few persistent launches as the partial-tile memory allows (jobs of

@@ -1,134 +1,147 @@
 // Plain FP64 triple-product lag accumulation (the reference loop of
-// 4_fbe/amber.c:247-279 restated for the GPU in FP64), the deterministic lag
-// reduction shared with the mixed-precision path, and the FP64 triple sum
-// that gives calCR's normaliser (amber_funcs.c:451-457).
+// 4_fbe/amber.c:247-279 / amber_v2.c:243-270 restated for the GPU in FP64), the
+// per-anchor lag reduction still used by the split-BF16 comparison path, and the
+// FP64 triple sum that gives calCR's normaliser (amber_funcs.c:451-457).
 //
-// For a triangle (r1, r2, r3) with maps D1, D2, D3 [channel][pixel] the
-// reference sums, over every admissible channel triplet (p1, p2, p3) with
-// |p2−p1|, |p3−p1| ≤ nc10, Σ_x D1[p1,x]·D2[p2,x]·D3[p3,x] into the lag cell
-// (p2−p1+nc10, p3−p1+nc10).  For one anchor p1 that is the matrix
-// T_p1 = (D2 ∘ D1[p1])·D3ᵀ restricted to the p1 window.  Each CTA here owns a
-// 64 × 64 tile of one anchor's window over one pixel range: it stages
-// D1[p1]·D2 and D3 for 16 pixels at a time in shared memory and accumulates a
-// 4 × 4 register block per thread in FP64.  Channel multiplicities
-// (flagging) weight the tile when it is written.  Tiles go to a partial
-// buffer [anchor][k-split][lag2][lag3]; lag_reduce sums that buffer per lag
-// cell in a fixed grouping and order with compensated (TwoSum) accumulators,
-// so results are deterministic.
+// The contraction is the lag-space GEMM of lagspace.cuh: per unit (a tile pair,
+// an anchor block and a run of pixel blocks) one CTA of 256 threads holds a
+// 128 × 128 FP64 accumulator tile, 8 × 8 per thread (rows ty·8 + i, columns
+// tx + 16·j, so that a warp's B reads are 16 consecutive doubles).  Per stage of
+// 16 pixels it copies the channel rows the unit's anchors touch — w·D1 of the
+// anchor block, w·D3 and w·D2 of the spans their windows cover — into shared
+// memory once (transposed, [pixel][channel]), then for every anchor group forms
+// the A operand D1[p1]·D3[p1 − nc10 + Δ3] (one multiply per element) and runs
+// 16 rank-1 steps of 64 FMAs per thread, reading B straight from the staged D2
+// rows at the group's window offset.  The FP64 sums never leave registers
+// until the unit's end; its partial tile is then summed per lag cell by
+// ls_reduce in a fixed order.
 #include <algorithm>
 
-#include "common.cuh"
+#include "lagspace.cuh"
 
 namespace amber {
 
 namespace {
 
-constexpr int TT = 64;  // tile edge in channels
-constexpr int KB = 16;  // pixels per shared-memory stage
+constexpr int F_KX = 16;   // pixels per stage
+constexpr int F_NT = 256;  // threads per CTA
 
-__global__ void __launch_bounds__(256) contract64_kernel(const double *__restrict__ m1, const double *__restrict__ m2,
-                                                          const double *__restrict__ m3, long k, long kp,
-                                                          const int *__restrict__ anchors,
-                                                          const int *__restrict__ weight, int nc, int nc10, int tiles,
-                                                          long kchunk, int use_abs, double *__restrict__ partial)
+struct F64Desc {
+    const double *m1, *m2, *m3;  // ring maps of r1, r2, r3 [nc][kp]
+    const int *weight;           // channel multiplicities [nc]
+    const int *groups;           // anchor groups, concatenated over anchor blocks
+    const int *group_off;        // [nab + 1]
+    long k, kp;
+    int nc, nc10, nclen, ks, AB;
+};
+
+// Shared-memory doubles of one stage for the largest staging the plan allows (row strides odd,
+// so that the transposed stores of 16 consecutive pixels hit 16 different bank pairs).
+constexpr int F_S1 = LS_ROWS * 2 + 1;  // D1 rows of an anchor block (AB ≤ 256 for k > 1)
+constexpr int F_S3 = LS_SPAN + 1;      // D3 span
+constexpr int F_S2 = LS_SPAN + 1;      // D2 span
+constexpr size_t F_SMEM = sizeof(double) * ((size_t)F_KX * (F_S1 + F_S3 + F_S2) + 2 * F_KX * LS_ROWS);
+
+__global__ void __launch_bounds__(F_NT, 1) ls_fp64_kernel(const F64Desc *__restrict__ jobs,
+                                                          const LsUnit *__restrict__ units,
+                                                          double *__restrict__ partial, int use_abs)
 {
-    // rows padded by 2 doubles: the transposed stores hit 8 distinct bank pairs
-    __shared__ __align__(16) double As[2][KB][TT + 2];
-    __shared__ __align__(16) double Bs[2][KB][TT + 2];
-    const int tid = threadIdx.x;
-    const int a = blockIdx.y, ks = blockIdx.z, KS = gridDim.z;
-    const int t2 = blockIdx.x / tiles, t3 = blockIdx.x % tiles;
-    const int p1 = anchors[a];
-    const int nclen = 2 * nc10 + 1;
-    const int d2b = TT * t2, d3b = TT * t3;
-    const int tx = tid & 15, ty = tid >> 4;
-    double *out = partial + ((size_t)a * KS + ks) * nclen * nclen;
+    extern __shared__ __align__(16) double sm[];
+    double *st1 = sm;                    // [F_KX][F_S1]  w·D1 of the anchor block
+    double *st3 = st1 + F_KX * F_S1;     // [F_KX][F_S3]  w·D3 of the span
+    double *st2 = st3 + F_KX * F_S3;     // [F_KX][F_S2]  w·D2 of the span
+    double *As = st2 + F_KX * F_S2;      // [2][F_KX][LS_ROWS] the formed A operand
 
-    // rows (p2) and columns (p3) this tile covers; -1 marks an empty row/col
-    __shared__ int prow[TT], pcol[TT];
-    __shared__ int any_row, any_col;
-    if (tid == 0) { any_row = 0; any_col = 0; }
-    __syncthreads();
-    if (tid < TT) {
-        int d = d2b + tid, p = p1 - nc10 + d;
-        bool ok = d < nclen && p >= 0 && p < nc && weight[p] > 0;
-        prow[tid] = ok ? p : -1;
-        if (ok) atomicOr(&any_row, 1);
-    } else if (tid < 2 * TT) {
-        int d = d3b + tid - TT, p = p1 - nc10 + d;
-        bool ok = d < nclen && p >= 0 && p < nc && weight[p] > 0;
-        pcol[tid - TT] = ok ? p : -1;
-        if (ok) atomicOr(&any_col, 1);
-    }
-    __syncthreads();
+    const LsUnit u = units[blockIdx.x];
+    const F64Desc j = jobs[u.job];
+    const int tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
+    const int ks = j.ks, nclen = j.nclen, nc = j.nc;
+    const int c0 = u.ab * j.AB, c1 = min(nc, c0 + j.AB), nab1 = c1 - c0;
+    const int mrows = ks > 1 ? ks * nclen : min(LS_ROWS, nclen - LS_ROWS * u.t3);
+    const int ncols = ks > 1 ? nclen + ks - 1 : min(LS_ROWS, nclen - LS_ROWS * u.t2);
+    const int row0_3 = c0 - j.nc10 + (ks > 1 ? 0 : LS_ROWS * u.t3);  // channel of staged D3 row 0
+    const int row0_2 = c0 - j.nc10 + (ks > 1 ? 0 : LS_ROWS * u.t2);  // channel of staged D2 row 0
+    const int span3 = nab1 + (ks > 1 ? nclen : mrows) - 1;
+    const int span2 = nab1 + ncols - 1;
+    const int g0 = j.group_off[u.ab], g1 = j.group_off[u.ab + 1];
 
-    double acc[4][4];
+    double acc[8][8];
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
+    for (int i = 0; i < 8; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+        for (int q = 0; q < 8; ++q) acc[i][q] = 0.0;
 
-    const long x0 = (long)ks * kchunk, x1 = min(k, x0 + kchunk);
-    if (any_row && any_col && x0 < x1) {
-        const double *c1 = m1 + (long)p1 * kp;
-        // each thread loads 4 elements of A and 4 of B per stage
-        auto load = [&](int buf, long xs) {
-#pragma unroll
-            for (int i = 0; i < 4; ++i) {
-                int e = tid + i * 256;
-                int r = e / KB, xx = e % KB;
-                long x = xs + xx;
-                double va = 0.0, vb = 0.0;
-                if (x < x1) {
-                    int pr = prow[r], pc = pcol[r];
-                    double s1 = c1[x];
-                    if (pr >= 0) va = s1 * m2[(long)pr * kp + x];
-                    if (pc >= 0) vb = m3[(long)pc * kp + x];
-                    if (use_abs) {
-                        va = fabs(va);
-                        vb = fabs(vb);
-                    }
+    // stage rows [0, n) of map m starting at channel ch0, weighted, into st[x][row]
+    auto stage = [&](double *st, int stride, const double *m, int ch0, int n, long x0) {
+        for (int e = tid; e < n * F_KX; e += F_NT) {
+            const int row = e / F_KX, xx = e % F_KX;
+            const int ch = ch0 + row;
+            const long x = x0 + xx;
+            double v = 0.0;
+            if (ch >= 0 && ch < nc && x < j.k) {
+                const int w = j.weight[ch];
+                if (w) {
+                    v = (double)w * m[(long)ch * j.kp + x];
+                    if (use_abs) v = fabs(v);
                 }
-                As[buf][xx][r] = va;
-                Bs[buf][xx][r] = vb;
             }
-        };
-        int buf = 0;
-        load(0, x0);
-        __syncthreads();
-        for (long xs = x0; xs < x1; xs += KB) {
-            if (xs + KB < x1) load(buf ^ 1, xs + KB);
+            st[xx * stride + row] = v;
+        }
+    };
+
+    int buf = 0;
+    for (long b = u.b0; b < u.b1; ++b) {
+        const long xb = b * LS_BLOCK;
+        for (long x0 = xb; x0 < min(j.k, xb + LS_BLOCK); x0 += F_KX) {
+            __syncthreads();  // the previous stage's readers are done
+            stage(st1, F_S1, j.m1, c0, nab1, x0);
+            stage(st3, F_S3, j.m3, row0_3, span3, x0);
+            stage(st2, F_S2, j.m2, row0_2, span2, x0);
+            for (int g = g0; g < g1; ++g) {
+                const int pb = j.groups[g];
+                // A[x][r] = D1[p1, x] · D3[p1 − nc10 + Δ3, x] for slot a and lag Δ3 of row r
+                __syncthreads();  // stage visible; A[buf] no longer read by the group before last
+                double *A = As + buf * (F_KX * LS_ROWS);
+                for (int e = tid; e < F_KX * LS_ROWS; e += F_NT) {
+                    const int r = e % LS_ROWS, xx = e / LS_ROWS;
+                    double v = 0.0;
+                    if (r < mrows) {
+                        const int a = ks > 1 ? r / nclen : 0, d3 = ks > 1 ? r % nclen : r;
+                        const int p1 = pb + a;
+                        if (p1 < c1) v = st1[xx * F_S1 + (p1 - c0)] * st3[xx * F_S3 + (p1 - c0) + d3];
+                    }
+                    A[xx * LS_ROWS + r] = v;
+                }
+                __syncthreads();
+                const double *B = st2 + (pb - c0) + tx;  // column tx + 16q of the group's window
+#pragma unroll 4
+                for (int xx = 0; xx < F_KX; ++xx) {
+                    const double2 *ap = reinterpret_cast<const double2 *>(A + xx * LS_ROWS + ty * 8);
+                    const double2 a01 = ap[0], a23 = ap[1], a45 = ap[2], a67 = ap[3];
+                    const double av[8] = {a01.x, a01.y, a23.x, a23.y, a45.x, a45.y, a67.x, a67.y};
+                    double bv[8];
 #pragma unroll
-            for (int xx = 0; xx < KB; ++xx) {
-                double2 a01 = *reinterpret_cast<const double2 *>(&As[buf][xx][ty * 4]);
-                double2 a23 = *reinterpret_cast<const double2 *>(&As[buf][xx][ty * 4 + 2]);
-                double2 b01 = *reinterpret_cast<const double2 *>(&Bs[buf][xx][tx * 4]);
-                double2 b23 = *reinterpret_cast<const double2 *>(&Bs[buf][xx][tx * 4 + 2]);
-                double av[4] = {a01.x, a01.y, a23.x, a23.y};
-                double bv[4] = {b01.x, b01.y, b23.x, b23.y};
+                    for (int q = 0; q < 8; ++q) bv[q] = B[xx * F_S2 + 16 * q];
 #pragma unroll
-                for (int i = 0; i < 4; ++i)
+                    for (int i = 0; i < 8; ++i)
 #pragma unroll
-                    for (int j = 0; j < 4; ++j) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
+                        for (int q = 0; q < 8; ++q) acc[i][q] = fma(av[i], bv[q], acc[i][q]);
+                }
+                buf ^= 1;
             }
-            __syncthreads();
-            buf ^= 1;
         }
     }
-    const double w1 = (double)weight[p1];
+    // the unit's partial tile [column][row]; slot a of a packed tile lands at lag column c − a
+    double *out = partial + u.tile * (long)(LS_ROWS * LS_ROWS);
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        int r = ty * 4 + i, d2 = d2b + r;
-        if (d2 >= nclen) continue;
-        int pr = prow[r];
-        double wr = pr >= 0 ? w1 * (double)weight[pr] : 0.0;
+    for (int i = 0; i < 8; ++i) {
+        const int r = ty * 8 + i;
+        if (r >= mrows) continue;
+        const int a = ks > 1 ? r / nclen : 0;
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            int cc = tx * 4 + j, d3 = d3b + cc;
-            if (d3 >= nclen) continue;
-            int pc = pcol[cc];
-            double wc = pc >= 0 ? (double)weight[pc] : 0.0;
-            out[(long)d2 * nclen + d3] = acc[i][j] * wr * wc;
+        for (int q = 0; q < 8; ++q) {
+            const int col = tx + 16 * q - a;
+            if (col >= 0 && col < (ks > 1 ? nclen : ncols)) out[(long)col * LS_ROWS + r] = acc[i][q];
         }
     }
 }
@@ -233,34 +246,105 @@ int lag_reduce(amber_cuda_ctx *c, const double *partial, long nunits, long ncsiz
     return cuda_check(c, cudaGetLastError(), "lag reduction launch");
 }
 
+int contract_fp64_jobs(amber_cuda_ctx *c, const std::vector<F64Job> &jobs)
+{
+    int rc;
+    if (jobs.empty()) return AMBER_OK;
+    const int nclen = 2 * c->nc10 + 1;
+    const long ncsize = (long)nclen * nclen;
+    const int nA = (int)c->anchors.size();
+    if (nA == 0) {
+        for (const F64Job &jb : jobs)
+            if ((rc = cuda_check(c, cudaMemsetAsync(jb.lag_out, 0, sizeof(double) * ncsize, c->stream), "zero lag")))
+                return rc;
+        return AMBER_OK;
+    }
+    constexpr size_t TILE_B = sizeof(double) * LS_ROWS * LS_ROWS;
+    const size_t pcap = std::max<size_t>((size_t)256 << 20, contract_partial_cap(c));
+    size_t j0 = 0;
+    while (j0 < jobs.size()) {
+        // plan as many jobs as their partial tiles allow in one launch
+        std::vector<LsJobPlan> plans;
+        long tiles = 0;
+        size_t j1 = j0;
+        for (; j1 < jobs.size(); ++j1) {
+            LsJobPlan p;
+            ls_plan_job(p, (int)c->nc, c->nc10, jobs[j1].k, c->weight, c->num_sms);
+            if (j1 > j0 && (size_t)(tiles + p.s.units()) * TILE_B > pcap) break;
+            p.unit_base = tiles;
+            tiles += p.s.units();
+            plans.push_back(std::move(p));
+        }
+        std::vector<LsUnit> units;
+        for (size_t i = 0; i < plans.size(); ++i) ls_units(plans[i], (int)i, units);
+        // largest units first, so that the small ones fill the tail of the launch
+        std::stable_sort(units.begin(), units.end(), [](const LsUnit &a, const LsUnit &b) { return a.work > b.work; });
+        // device: descriptors, units and anchor groups, through the pinned staging area
+        size_t ngroups = 0, noff = 0;
+        for (const LsJobPlan &p : plans) {
+            ngroups += p.groups.size();
+            noff += p.group_off.size();
+        }
+        const size_t desc_b = sizeof(F64Desc) * plans.size(), unit_b = sizeof(LsUnit) * units.size();
+        const size_t off_u = (desc_b + 255) / 256 * 256, off_g = off_u + (unit_b + 255) / 256 * 256;
+        const size_t off_o = off_g + (sizeof(int) * ngroups + 255) / 256 * 256;
+        const size_t stage_b = off_o + sizeof(int) * noff;
+        if ((rc = ensure(c, c->partial, (size_t)tiles * TILE_B, "partial lag tiles"))) return rc;
+        if ((rc = ensure(c, c->jobdesc, stage_b, "job list"))) return rc;
+        if ((rc = cuda_check(c, cudaStreamSynchronize(c->stream), "job staging"))) return rc;
+        if (c->stage_bytes < stage_b) {
+            if (c->stage) cudaFreeHost(c->stage);
+            c->stage = nullptr;
+            c->stage_bytes = 0;
+            if ((rc = cuda_check(c, cudaHostAlloc(&c->stage, stage_b, cudaHostAllocDefault), "job staging"))) return rc;
+            c->stage_bytes = stage_b;
+        }
+        char *h = (char *)c->stage, *d = (char *)c->jobdesc.p;
+        F64Desc *hd = (F64Desc *)h;
+        int *hg = (int *)(h + off_g), *ho = (int *)(h + off_o);
+        std::vector<LsReduceJob> red;
+        size_t gpos = 0, opos = 0;
+        for (size_t i = 0; i < plans.size(); ++i) {
+            const F64Job &jb = jobs[j0 + i];
+            const LsJobPlan &p = plans[i];
+            F64Desc &x = hd[i];
+            x.m1 = jb.m1; x.m2 = jb.m2; x.m3 = jb.m3;
+            x.weight = (const int *)c->d_weight.p;
+            x.groups = (const int *)(d + off_g) + gpos;
+            x.group_off = (const int *)(d + off_o) + opos;
+            x.k = jb.k; x.kp = jb.kp;
+            x.nc = (int)c->nc; x.nc10 = c->nc10; x.nclen = nclen; x.ks = p.s.k; x.AB = p.s.AB;
+            std::copy(p.groups.begin(), p.groups.end(), hg + gpos);
+            for (size_t q = 0; q < p.group_off.size(); ++q) ho[opos + q] = p.group_off[q];
+            gpos += p.groups.size();
+            opos += p.group_off.size();
+            red.push_back(LsReduceJob{(const double *)c->partial.p + p.unit_base * LS_ROWS * LS_ROWS, jb.lag_out, nclen,
+                                      p.s.k, p.s.T, p.s.nab, p.s.V});
+        }
+        std::copy(units.begin(), units.end(), (LsUnit *)(h + off_u));
+        if ((rc = cuda_check(c, cudaMemcpyAsync(d, h, stage_b, cudaMemcpyHostToDevice, c->stream), "job list upload")))
+            return rc;
+        cudaFuncSetAttribute(ls_fp64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)F_SMEM);
+        phase_begin(c, 1);
+        for (size_t u0 = 0; u0 < units.size(); u0 += 1u << 30) {
+            const unsigned n = (unsigned)std::min<size_t>(units.size() - u0, 1u << 30);
+            ls_fp64_kernel<<<n, F_NT, F_SMEM, c->stream>>>((const F64Desc *)d, (const LsUnit *)(d + off_u) + u0,
+                                                          (double *)c->partial.p, c->fp64_abs ? 1 : 0);
+            c->launches += 1;
+            c->contractions += 1;
+        }
+        phase_end(c);
+        if ((rc = cuda_check(c, cudaGetLastError(), "ls_fp64_kernel launch"))) return rc;
+        if ((rc = ls_reduce(c, red))) return rc;
+        j0 = j1;
+    }
+    return AMBER_OK;
+}
+
 int contract_fp64(amber_cuda_ctx *c, const double *m1, const double *m2, const double *m3, long k, long kp,
                   double *lag_out)
 {
-    const int nc10 = c->nc10;
-    const int nclen = 2 * nc10 + 1;
-    const long ncsize = (long)nclen * nclen;
-    const int nA = (int)c->anchors.size();
-    if (nA == 0) return cuda_check(c, cudaMemsetAsync(lag_out, 0, sizeof(double) * ncsize, c->stream), "zero lag");
-    const int tiles = (nclen + TT - 1) / TT;
-    long blocks = (long)tiles * tiles * nA;
-    long want = 4L * c->num_sms;
-    int KS = (int)std::max<long>(1, std::min<long>((want + blocks - 1) / blocks, (k + 1023) / 1024));
-    long kchunk = ((k + KS - 1) / KS + KB - 1) / KB * KB;
-    KS = (int)((k + kchunk - 1) / kchunk);
-    if (KS < 1) KS = 1;
-    size_t pbytes = sizeof(double) * (size_t)nA * KS * ncsize;
-    int rc = ensure(c, c->partial, pbytes, "partial lag tiles");
-    if (rc) return rc;
-    dim3 grid((unsigned)(tiles * tiles), (unsigned)nA, (unsigned)KS);
-    phase_begin(c, 1);
-    contract64_kernel<<<grid, 256, 0, c->stream>>>(m1, m2, m3, k, kp, (const int *)c->d_anchors.p,
-                                                   (const int *)c->d_weight.p, (int)c->nc, nc10, tiles, kchunk,
-                                                   c->fp64_abs ? 1 : 0, (double *)c->partial.p);
-    phase_end(c);
-    c->launches += 1;
-    c->contractions += 1;
-    if ((rc = cuda_check(c, cudaGetLastError(), "contract64_kernel launch"))) return rc;
-    return lag_reduce(c, (const double *)c->partial.p, (long)nA * KS, ncsize, lag_out);
+    return contract_fp64_jobs(c, {F64Job{m1, m2, m3, k, kp, lag_out}});
 }
 
 int triple_sums(amber_cuda_ctx *c, const double *maps, long n, const std::vector<int> &tri, double *out)

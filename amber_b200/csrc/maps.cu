@@ -32,7 +32,7 @@
 #include <algorithm>
 #include <vector>
 
-#include "common.cuh"
+#include "lagspace.cuh"
 
 namespace amber {
 
@@ -177,7 +177,7 @@ __global__ void __launch_bounds__(kThreads) ring_rows_kernel(const double2 *__re
                                                               uint16_t *__restrict__ out_hi,
                                                               uint16_t *__restrict__ out_lo,
                                                               float *__restrict__ out_f32,
-                                                              unsigned *__restrict__ rowmax)
+                                                              const int *__restrict__ weight)
 {
     extern __shared__ double2 smem[];
     double2 *tw = smem;       // ng
@@ -208,7 +208,8 @@ __global__ void __launch_bounds__(kThreads) ring_rows_kernel(const double2 *__re
     const int ngroups = (kThreads / 32) * G;
     const long npair = ng / 2 + 1;
     const long slot_row = ((long)s * nch + q0 + q) * kp + n0 * ng;
-    float amax = 0.f;  // max |fp32 value| this thread writes (row exponent for the int8 digits)
+    // the mixed path's fp32 maps carry the channel multiplicity (0 for flagged channels)
+    const double wq = (weight && q0 + q < nch) ? (double)weight[q0 + q] : 1.0;
     for (long nb = gid; nb * R < npair; nb += ngroups) {
         double acc[R], accm[R];  // pixel x, pixel Ng − x
         int idx[R], step[R];
@@ -245,11 +246,7 @@ __global__ void __launch_bounds__(kThreads) ring_rows_kernel(const double2 *__re
                     const long o = slot_row + n1;
                     const double v = h == 0 ? acc[r] : accm[r];
                     if (out_f64) out_f64[o] = v;
-                    if (out_f32) {
-                        float f = (float)v;
-                        out_f32[o] = f;
-                        amax = fmaxf(amax, fabsf(f));
-                    }
+                    if (out_f32) out_f32[o] = (float)(v * wq);
                     if (out_hi) {
                         // split: hi = bf16(v), lo = bf16(v − hi) (both round-to-nearest)
                         float f = (float)v;
@@ -262,13 +259,18 @@ __global__ void __launch_bounds__(kThreads) ring_rows_kernel(const double2 *__re
             }
         }
     }
-    if (rowmax && q0 + q < nch) atomicMax(&rowmax[(long)s * nch + q0 + q], __float_as_uint(amax));
 }
 
-// Fixed-point digits of one map row for the int8 tensor-core contraction.
-// E is the smallest exponent with max|v| < 2^E; then, with base 254,
+// Fixed-point digits for the int8 tensor-core contraction.  Every block of
+// LS_BLOCK pixels of a ring slot has one exponent E, shared by all channels:
+// the smallest with max|v| < 2^E over the block (0 for an all-zero block).
+// Then, with base 254,
 //     v·2^−E·127 = d0 + d1/254 + d2/254² + r,   d0, d1, d2 ∈ [−127, 127],
 // |r| ≤ 1/(2·254²): signed, balanced digits that use the whole int8 range.
+// An exponent per pixel block (rather than per channel row) is what lets the
+// contraction add every anchor into one accumulator (lagspace.cuh), and it
+// follows the maps' spatial dynamic range: the sampling-mask maps are sharply
+// peaked at the origin, so blocks far from it get a much finer digit scale.
 __device__ __forceinline__ void digits254(float t, uint32_t &b0, uint32_t &b1, uint32_t &b2)
 {
     // round-to-nearest via the 1.5·2^23 magic number: the integer sits in the
@@ -284,28 +286,57 @@ __device__ __forceinline__ void digits254(float t, uint32_t &b0, uint32_t &b1, u
     b2 = __float_as_uint(y2);
 }
 
-__global__ void quantize_kernel(const float *__restrict__ f32, const unsigned *__restrict__ rowmax, long k, long kp,
-                                long nrows, int8_t *__restrict__ d0, int8_t *__restrict__ d1, int8_t *__restrict__ d2,
-                                int *__restrict__ expo)
+// bexp[s][b] for block b of slot s (one CTA of LS_BLOCK threads per block: a thread per pixel,
+// looping over the channels, so every channel row is read coalesced).
+__global__ void __launch_bounds__(LS_BLOCK) block_expo_kernel(const float *__restrict__ f32, long k, long kp,
+                                                              long nch, long nblk, int *__restrict__ bexp)
 {
-    const long row = blockIdx.y;
-    const float mx = __uint_as_float(rowmax[row]);
-    const int E = mx > 0.f ? ilogbf(mx) + 1 : 0;
-    if (blockIdx.x == 0 && threadIdx.x == 0) expo[row] = E;
-    const float sc = ldexpf(127.f, -E);
-    for (long x4 = (long)blockIdx.x * blockDim.x + threadIdx.x; x4 * 4 < kp; x4 += (long)gridDim.x * blockDim.x) {
-        uint32_t a[4], b[4], c[4];
+    __shared__ float red[LS_BLOCK / 32];
+    const long b = blockIdx.x;
+    const int s = blockIdx.y;
+    const long x = b * LS_BLOCK + threadIdx.x;
+    float m = 0.f;
+    if (x < k)
+        for (long ch = 0; ch < nch; ++ch) m = fmaxf(m, fabsf(f32[((long)s * nch + ch) * kp + x]));
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < LS_BLOCK / 32; ++w) m = fmaxf(m, red[w]);
+        bexp[(long)s * nblk + b] = m > 0.f ? ilogbf(m) + 1 : 0;
+    }
+}
+
+// Three digit planes per slot in the contraction's staging order,
+// dig[s][digit][x/16][ch][16 pixels]: a TMA box of consecutive channels and two 16-pixel
+// groups then lands in shared memory exactly as the MMA reads a K-major operand without
+// swizzle (8-row core matrices of 16 bytes).  Pixels at or past k become zero digits.
+__global__ void __launch_bounds__(256) quantize_kernel(const float *__restrict__ f32, const int *__restrict__ bexp,
+                                                       long k, long kp, long nch, long nblk,
+                                                       int8_t *__restrict__ dig)
+{
+    const long b = blockIdx.x;
+    const int s = blockIdx.y;
+    const float sc = ldexpf(127.f, -bexp[(long)s * nblk + b]);
+    const long kpg = kp / 16;
+    for (long e = threadIdx.x; e < (LS_BLOCK / 16) * nch; e += blockDim.x) {
+        const long g = e / nch, ch = e % nch;
+        const long x0 = b * LS_BLOCK + g * 16;
+        const float *src = f32 + ((long)s * nch + ch) * kp + x0;
+        uint32_t w[3][4];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const long x = x4 * 4 + j;
-            digits254(x < k ? f32[row * kp + x] * sc : 0.f, a[j], b[j], c[j]);
+        for (int q = 0; q < 4; ++q) {
+            uint32_t a[4], bb[4], cc[4];
+#pragma unroll
+            for (int t = 0; t < 4; ++t) digits254(x0 + 4 * q + t < k ? src[4 * q + t] * sc : 0.f, a[t], bb[t], cc[t]);
+            w[0][q] = __byte_perm(__byte_perm(a[0], a[1], 0x0040), __byte_perm(a[2], a[3], 0x0040), 0x5410);
+            w[1][q] = __byte_perm(__byte_perm(bb[0], bb[1], 0x0040), __byte_perm(bb[2], bb[3], 0x0040), 0x5410);
+            w[2][q] = __byte_perm(__byte_perm(cc[0], cc[1], 0x0040), __byte_perm(cc[2], cc[3], 0x0040), 0x5410);
         }
-        reinterpret_cast<uint32_t *>(d0 + row * kp)[x4] =
-            __byte_perm(__byte_perm(a[0], a[1], 0x0040), __byte_perm(a[2], a[3], 0x0040), 0x5410);
-        reinterpret_cast<uint32_t *>(d1 + row * kp)[x4] =
-            __byte_perm(__byte_perm(b[0], b[1], 0x0040), __byte_perm(b[2], b[3], 0x0040), 0x5410);
-        reinterpret_cast<uint32_t *>(d2 + row * kp)[x4] =
-            __byte_perm(__byte_perm(c[0], c[1], 0x0040), __byte_perm(c[2], c[3], 0x0040), 0x5410);
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+            *reinterpret_cast<uint4 *>(dig + (((long)s * 3 + d) * kpg + x0 / 16) * nch * 16 + ch * 16) =
+                make_uint4(w[d][0], w[d][1], w[d][2], w[d][3]);
     }
 }
 
@@ -404,7 +435,7 @@ int build_maps(amber_cuda_ctx *c, const MapJob &job)
         cudaFuncSetAttribute(ring_rows_kernel<CC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s2);        \
         ring_rows_kernel<CC><<<g2, kThreads, s2, c->stream>>>(Y, ng, jmax, d_jc, job.nch, tw, job.kp,          \
                                                                job.out_f64, job.out_hi, job.out_lo, job.out_f32,  \
-                                                               job.rowmax);                                       \
+                                                               job.weight);                                       \
     } while (0)
     switch (C2) {
         case 32: LAUNCH_ROWS(32); break;
@@ -417,12 +448,12 @@ int build_maps(amber_cuda_ctx *c, const MapJob &job)
 #undef LAUNCH_ROWS
     c->launches += 1;
     if ((rc = cuda_check(c, cudaGetLastError(), "ring_rows_kernel launch"))) return rc;
-    if (job.d0) {
-        const long nrows = (long)job.nslots * job.nch;
-        dim3 gq((unsigned)std::min<long>((job.kp / 4 + 255) / 256, 64), (unsigned)nrows);
-        quantize_kernel<<<gq, 256, 0, c->stream>>>(job.out_f32, job.rowmax, ng * ng, job.kp, nrows, job.d0, job.d1,
-                                                   job.d2, job.expo);
-        c->launches += 1;
+    if (job.dig) {
+        const long nblk = job.kp / LS_BLOCK;
+        dim3 gq((unsigned)nblk, (unsigned)job.nslots);
+        block_expo_kernel<<<gq, LS_BLOCK, 0, c->stream>>>(job.out_f32, ng * ng, job.kp, job.nch, nblk, job.bexp);
+        quantize_kernel<<<gq, 256, 0, c->stream>>>(job.out_f32, job.bexp, ng * ng, job.kp, job.nch, nblk, job.dig);
+        c->launches += 2;
         rc = cuda_check(c, cudaGetLastError(), "quantize_kernel launch");
     }
     return rc;

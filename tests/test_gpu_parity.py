@@ -144,67 +144,50 @@ def test_isosceles_symmetry_full_size(lib_built):
             assert (np.abs(nt[i] - nt[i].T) <= tol * at[i] + 1e-300).all(), prec
 
 
-def test_split_anchor_groups_match(lib_built):
-    """A job whose partial tiles exceed the per-launch cap runs as anchor groups whose lag sums add
-    up in order.  128-pixel chunks on the Ng1 = 354 triangle of the single-realisation workload
-    make its partial tiles ~14 GB (the cap is at most 8 GB): the result must equal the default
-    chunking's up to the FP64 summation order."""
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_unit_size_changes_only_rounding(precision, lib_built):
+    """The contraction's work units (runs of 256-pixel blocks, each summed into a partial tile of
+    its own) set only the FP64 summation grouping.  One-block units (chunk_px = 256) on the
+    Ng1 = 354 triangle of the single-realisation workload (490 blocks) against the default units:
+    counts identical, lag arrays equal to FP64 rounding."""
     import amber_b200
     real = synth.config2(seed=1)
     out = []
-    for chunk_px in (0, 128):
-        with amber_b200.Estimator(precision="mixed", chunk_px=chunk_px) as est:
+    for chunk_px in (0, 256):
+        with amber_b200.Estimator(precision=precision, chunk_px=chunk_px) as est:
             est.load_grid(real.gv, real.counts, real.du, real.flag_key)
             est.set_rings(real.ulow, real.uhigh)
             est.set_channels(real.nc10, real.uf_chans)
             tri = est.calcr()[:, :3].astype(np.int32)
             est.run(tri[[140]], want_v2=True)
             out.append(est.fetch(want_v2=True))
-            n_launch = est.last_run_breakdown()[4]
     (b0, n0, t0), (b1, n1, t1) = out
-    assert n_launch >= 4  # two anchor groups per pass
     np.testing.assert_array_equal(n0, n1)
     np.testing.assert_allclose(b1, b0, rtol=0, atol=1e-12 * np.abs(b0).max())
     np.testing.assert_allclose(t1, t0, rtol=0, atol=1e-12 * np.abs(t0).max())
 
 
-def test_tile_width_is_numerically_neutral(lib_built):
-    """The autotuner may pick either p3 tile width for 32 < nclen <= 128: the int8 digit products
-    accumulate exactly and the chunking is planned independently of the width, so forced 32,
-    forced 64 and the tuned choice give bit-identical lag arrays."""
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("nn,nc,nbins,hi,nc10,flagged,seed", [
+    (32, 100, 2, 10.0, 40, [5, 50], 54),                         # nclen = 81: one tile, no anchor packing
+    (32, 150, 2, 10.0, 70, [3, 77, 149], 53),                    # nclen = 141: 2 × 2 tiles, two anchor blocks
+    (32, 140, 2, 10.0, 60, list(range(128, 140)), 55),           # the second anchor block has no anchors
+])
+def test_estimator_vs_oracle_wide_windows(precision, nn, nc, nbins, hi, nc10, flagged, seed, lib_built):
+    """Lag windows wider than one 64-row anchor packing: a single 128-row tile, a 2 × 2 tile grid with
+    channels in two anchor blocks, and an anchor block whose channels are all flagged."""
     import amber_b200
-    real = synth.tiny(64, 40, seed=52, nbins=6, hi=28.0, nc10=19, flagged=[0, 39])
-    outs = []
-    for tile_n in (32, 64, 0):
-        with amber_b200.Estimator(precision="mixed", tile_n=tile_n) as est:
-            amber_b200.estimate(real, precision="mixed", version=2, est=est)
-            outs.append(est.fetch(want_v2=True))
-            if tile_n == 0:
-                ch = est.tile_choices()
-    assert 40 in ch and ch[40][0] in (32, 64)
-    for o in outs[1:]:
-        for a, b in zip(outs[0], o):
-            np.testing.assert_array_equal(a, b)
-
-
-def test_ss_tile_is_bit_identical(lib_built):
-    """tile_n = 128 runs the contraction with both MMA operands in shared memory (N = 128, 64-pixel
-    stages): the same digit arithmetic and chunking, so its lag arrays equal the 64-wide path's bit
-    for bit — one tile (nclen = 39) and a 2 × 2 tile grid (nclen = 141, rows and pixels past the
-    ends, flagged channels)."""
-    import amber_b200
-    cases = [(synth.tiny(64, 40, seed=52, nbins=6, hi=28.0, nc10=19, flagged=[0, 39]), 0),
-             (synth.tiny(96, 150, seed=53, nbins=5, hi=40.0, nc10=70, flagged=[3, 77, 149]), 0),
-             (synth.tiny(32, 10, seed=54, nbins=4, hi=14.0, nc10=4), 0),     # nclen = 9: mostly idle columns
-             (synth.tiny(64, 40, seed=55, nbins=6, hi=28.0, nc10=19), 128)]  # 128-pixel chunks, ragged last
-    for real, chunk_px in cases:
-        outs = []
-        for tile_n in (64, 128):
-            with amber_b200.Estimator(precision="mixed", tile_n=tile_n, chunk_px=chunk_px) as est:
-                amber_b200.estimate(real, precision="mixed", version=2, est=est)
-                outs.append(est.fetch(want_v2=True))
-        for a, b in zip(*outs):
-            np.testing.assert_array_equal(a, b)
+    real = synth.tiny(nn, nc, seed=seed, nbins=nbins, hi=hi, nc10=nc10, flagged=flagged)
+    rdata, res = amber_b200.estimate(real, precision=precision, version=2)
+    ordata, ores = oracle.estimate(real, version=2, with_absscale=True)
+    np.testing.assert_array_equal(rdata[:, :3], ordata[:, :3])
+    tol = TOL[precision]
+    for r, o in zip(res, ores):
+        np.testing.assert_array_equal(r["numdnu"], o["numdnu"])
+        e = np.abs(r["bldnu"] - o["bldnu"]) / (o["absscale"] + 1e-300)
+        assert e.max() <= tol, e.max()
+        ei = np.abs(r["numtri"] - o["numtri"]) / (o["absscale_i"] + 1e-300)
+        assert ei.max() <= tol, ei.max()
 
 
 @pytest.mark.skipif(not oracle.ref_available(), reason="reference build (oracle/_ref) not present")
