@@ -33,7 +33,8 @@ PREC = {"fp64": 0, "mixed": 1, "bf16x3": 2, "fp64_abs": 3}
 # every entry point include/amber_cuda.h declares
 EXPORTS = (
     "amber_cuda_default_opts", "amber_cuda_create", "amber_cuda_destroy", "amber_cuda_last_error",
-    "amber_cuda_load_grid_packed", "amber_cuda_load_grid", "amber_cuda_set_rings", "amber_cuda_get_uavg",
+    "amber_cuda_load_grid_packed", "amber_cuda_load_grid", "amber_cuda_load_grid_device", "amber_cuda_set_rings",
+    "amber_cuda_get_uavg",
     "amber_cuda_set_channels", "amber_cuda_calcr", "amber_cuda_ng1", "amber_cuda_triangle_v1",
     "amber_cuda_triangle_v2", "amber_cuda_triangles", "amber_cuda_triangles_run", "amber_cuda_triangles_fetch",
     "amber_cuda_last_run_stats", "amber_cuda_last_run_breakdown", "amber_cuda_last_run_shape", "amber_cuda_grid_vis",
@@ -85,7 +86,7 @@ class Request(ctypes.Structure):
                 ("Nr", ctypes.c_int), ("ULow", ctypes.POINTER(ctypes.c_double)),
                 ("UHigh", ctypes.POINTER(ctypes.c_double)), ("nc10", ctypes.c_int), ("uf_nc", ctypes.c_int),
                 ("uf_chans", ctypes.POINTER(ctypes.c_int)), ("want_v2", ctypes.c_int),
-                ("cylbs", ctypes.POINTER(CylBsParams))]
+                ("cylbs", ctypes.POINTER(CylBsParams)), ("inputs_on_device", ctypes.c_int)]
 
 
 class EngineInfo(ctypes.Structure):
@@ -93,7 +94,8 @@ class EngineInfo(ctypes.Structure):
                 ("max_active", ctypes.c_long), ("queued", ctypes.c_long), ("active", ctypes.c_long),
                 ("peak_bytes", ctypes.c_size_t), ("budget_bytes", ctypes.c_size_t), ("products", ctypes.c_double),
                 ("busy_ms", ctypes.c_double), ("setup_ms", ctypes.c_double), ("maps_ms", ctypes.c_double),
-                ("contract_ms", ctypes.c_double), ("finish_ms", ctypes.c_double)]
+                ("contract_ms", ctypes.c_double), ("finish_ms", ctypes.c_double), ("kernel_launches", ctypes.c_long),
+                ("contract_kernel_ms", ctypes.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -228,6 +230,13 @@ class Estimator:
     def load_grid_raw(self, re_im_ptr: int, ntig_ptr: int, nn: int, nc: int, du: float, flag_key: int):
         """Same as load_grid but from raw host addresses (e.g. pinned buffers)."""
         self._check(self._L.amber_cuda_load_grid_packed(self._h, nn, nc, float(du), int(flag_key),
+                                                        ctypes.cast(re_im_ptr, _dp), ctypes.cast(ntig_ptr, _dp)))
+        self.n1, self.nc = nn, nc
+
+    def load_grid_device(self, re_im_ptr: int, ntig_ptr: int, nn: int, nc: int, du: float, flag_key: int):
+        """Same as load_grid_raw but from device addresses on this context's device (a cube kept
+        resident in HBM, e.g. torch tensors): normalised in place, nothing copied in."""
+        self._check(self._L.amber_cuda_load_grid_device(self._h, nn, nc, float(du), int(flag_key),
                                                         ctypes.cast(re_im_ptr, _dp), ctypes.cast(ntig_ptr, _dp)))
         self.n1, self.nc = nn, nc
 
@@ -401,17 +410,21 @@ class Estimator:
         return ri[..., 0] + 1j * ri[..., 1], nt
 
 
-def _request_of(real, want_v2, cyl=None):
+def _request_of(real, want_v2, cyl=None, with_cube=True):
     """Request struct for a synth.Realisation, with the numpy buffers it points to (keep them alive
     until enqueue returns: the library copies them)."""
-    ri = np.ascontiguousarray(real.gv, dtype=np.complex128).view(np.float64)
-    nt = np.ascontiguousarray(real.counts, dtype=np.float64)
+    if with_cube:
+        ri = np.ascontiguousarray(real.gv, dtype=np.complex128).view(np.float64)
+        nt = np.ascontiguousarray(real.counts, dtype=np.float64)
+    else:
+        ri = np.zeros(2)
+        nt = np.zeros(1)
     lo = np.ascontiguousarray(real.ulow, dtype=np.float64)
     hi = np.ascontiguousarray(real.uhigh, dtype=np.float64)
     uf = np.ascontiguousarray(real.uf_chans if real.flag_key == 1 else np.zeros(1), dtype=np.int32)
     q = Request(real.gv.shape[0], real.gv.shape[2], float(real.du), int(real.flag_key), _ptr(ri, _dp), _ptr(nt, _dp),
                 len(lo), _ptr(lo, _dp), _ptr(hi, _dp), int(real.nc10), len(uf) if real.flag_key == 1 else 0,
-                _ptr(uf, _ip), int(bool(want_v2)), None if cyl is None else ctypes.pointer(cyl))
+                _ptr(uf, _ip), int(bool(want_v2)), None if cyl is None else ctypes.pointer(cyl), 0)
     return q, (ri, nt, lo, hi, uf, cyl)
 
 
@@ -425,11 +438,18 @@ class Engine:
         self._L = est._L
         self._cyl_n = {}  # ticket -> N of the cylindrical bispectra it asked for
 
-    def enqueue(self, real, want_v2=True, cyl_bs=None) -> int:
+    def enqueue(self, real, want_v2=True, cyl_bs=None, device_cube=None) -> int:
         """Queue a realisation; ``cyl_bs`` (a dict of cylbs_params arguments, e.g.
-        ``dict(window=True, denominator="mask")``) asks for its cylindrical bispectra as well."""
+        ``dict(window=True, denominator="mask")``) asks for its cylindrical bispectra as well.
+        ``device_cube=(re_im_ptr, ntig_ptr)``: the realisation's summed grid and counts are already
+        in device memory (packed layout); the request reads them there, so keep them unchanged until
+        it is done."""
         cyl = None if cyl_bs is None else cylbs_params(**cyl_bs)
-        q, keep = _request_of(real, want_v2, cyl)
+        q, keep = _request_of(real, want_v2, cyl, with_cube=device_cube is None)
+        if device_cube is not None:
+            q.re_im = ctypes.cast(device_cube[0], _dp)
+            q.ntig = ctypes.cast(device_cube[1], _dp)
+            q.inputs_on_device = 1
         t = ctypes.c_int64()
         self.est._check(self._L.amber_cuda_enqueue(self.est._h, ctypes.byref(q), ctypes.byref(t)))
         del keep

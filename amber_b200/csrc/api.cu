@@ -165,7 +165,7 @@ int check_ready(amber_cuda_ctx *c, bool need_channels)
 }
 
 int upload_grid(amber_cuda_ctx *c, long N1, long nc, double Du, int flag_key, const double *re_im,
-                const double *ntig)
+                const double *ntig, bool on_device = false)
 {
     if (N1 <= 0 || N1 % 2 || nc <= 0 || !(Du > 0) || !re_im || !ntig)
         return fail(c, AMBER_ERR_ARG, "bad grid arguments (N1=%ld nc=%ld Du=%g)", N1, nc, Du);
@@ -174,16 +174,26 @@ int upload_grid(amber_cuda_ctx *c, long N1, long nc, double Du, int flag_key, co
     int rc;
     if ((rc = ensure(c, c->grid, sizeof(double2) * n, "grid"))) return rc;
     if ((rc = ensure(c, c->mask, sizeof(double) * n, "sampling mask"))) return rc;
-    // the raw sums land in the partial buffer first, then normalise into grid/mask
-    if ((rc = ensure(c, c->partial, sizeof(double2) * n + sizeof(double) * n, "grid staging"))) return rc;
-    double2 *raw = (double2 *)c->partial.p;
-    double *cnt = (double *)((char *)c->partial.p + sizeof(double2) * n);
-    if ((rc = cuda_check(c, cudaMemcpyAsync(raw, re_im, sizeof(double2) * n, cudaMemcpyHostToDevice, c->stream),
-                         "upload grid")))
-        return rc;
-    if ((rc = cuda_check(c, cudaMemcpyAsync(cnt, ntig, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream),
-                         "upload sampling")))
-        return rc;
+    const double2 *raw;
+    const double *cnt;
+    if (on_device) {
+        // normalised straight from the caller's device buffers
+        raw = (const double2 *)re_im;
+        cnt = ntig;
+    } else {
+        // the raw sums land in the partial buffer first, then normalise into grid/mask
+        if ((rc = ensure(c, c->partial, sizeof(double2) * n + sizeof(double) * n, "grid staging"))) return rc;
+        double2 *sraw = (double2 *)c->partial.p;
+        double *scnt = (double *)((char *)c->partial.p + sizeof(double2) * n);
+        if ((rc = cuda_check(c, cudaMemcpyAsync(sraw, re_im, sizeof(double2) * n, cudaMemcpyHostToDevice, c->stream),
+                             "upload grid")))
+            return rc;
+        if ((rc = cuda_check(c, cudaMemcpyAsync(scnt, ntig, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream),
+                             "upload sampling")))
+            return rc;
+        raw = sraw;
+        cnt = scnt;
+    }
     normalize_kernel<<<4 * c->num_sms, 256, 0, c->stream>>>(raw, cnt, n, (double2 *)c->grid.p, (double *)c->mask.p);
     if ((rc = cuda_check(c, cudaGetLastError(), "normalize launch"))) return rc;
     c->N1 = N1;
@@ -498,6 +508,22 @@ int amber_cuda_load_grid_packed(amber_cuda_ctx *c, long N1, long nc, double Du, 
     if (!c) return AMBER_ERR_ARG;
     cudaSetDevice(c->device);
     return upload_grid(c, N1, nc, Du, flag_key, re_im, ntig);
+}
+
+int amber_cuda_load_grid_device(amber_cuda_ctx *c, long N1, long nc, double Du, int flag_key, const double *re_im,
+                                const double *ntig)
+{
+    if (!c) return AMBER_ERR_ARG;
+    cudaSetDevice(c->device);
+    cudaPointerAttributes a{}, b{};
+    if (re_im && ntig &&
+        (cudaPointerGetAttributes(&a, re_im) != cudaSuccess || cudaPointerGetAttributes(&b, ntig) != cudaSuccess ||
+         a.type != cudaMemoryTypeDevice || b.type != cudaMemoryTypeDevice || a.device != c->device ||
+         b.device != c->device)) {
+        cudaGetLastError();
+        return fail(c, AMBER_ERR_ARG, "load_grid_device: re_im and ntig must be device memory of device %d", c->device);
+    }
+    return upload_grid(c, N1, nc, Du, flag_key, re_im, ntig, true);
 }
 
 int amber_cuda_load_grid(amber_cuda_ctx *c, long N1, long nc, double Du, int flag_key, const double *const *GVre,

@@ -4,17 +4,20 @@
 // FP64 triple sum that gives calCR's normaliser (amber_funcs.c:451-457).
 //
 // The contraction is the lag-space GEMM of lagspace.cuh: per unit (a tile pair,
-// an anchor block and a run of pixel blocks) one CTA of 256 threads holds a
-// 128 × 128 FP64 accumulator tile, 8 × 8 per thread (rows ty·8 + i, columns
-// tx + 16·j, so that a warp's B reads are 16 consecutive doubles).  Per stage of
-// 16 pixels it copies the channel rows the unit's anchors touch — w·D1 of the
-// anchor block, w·D3 and w·D2 of the spans their windows cover — into shared
-// memory once (transposed, [pixel][channel]), then for every anchor group forms
-// the A operand D1[p1]·D3[p1 − nc10 + Δ3] (one multiply per element) and runs
-// 16 rank-1 steps of 64 FMAs per thread, reading B straight from the staged D2
-// rows at the group's window offset.  The FP64 sums never leave registers
-// until the unit's end; its partial tile is then summed per lag cell by
-// ls_reduce in a fixed order.
+// an anchor block and a run of pixel blocks) one CTA of 8 warps holds a 128 × 128
+// FP64 accumulator tile in registers, 16 warps each holding a 32 × 32 block as
+// 4 × 4 fragments of the FP64 tensor-core MMA (mma.sync m8n8k4); four warps per
+// SM sub-partition keep its FP64 pipe fed.  Per stage of 16
+// pixels the CTA copies the channel rows its anchors touch — w·D1 of the anchor
+// block, w·D3 and w·D2 of the spans their windows cover — into shared memory
+// once (transposed, [pixel][channel]); then, for every anchor group, it forms
+// the A operand D1[p1]·D3[p1 − nc10 + Δ3] (one multiply per element, into one
+// of two buffers) and runs four k = 4 steps of 16 MMAs per warp, reading B
+// straight from the staged D2 rows at the group's window offset.  Row strides
+// of the A buffer and the D2 stage are ≡ 4 (mod 16) doubles, so a fragment
+// load (4 pixels × 8 rows) hits 16 distinct bank pairs per half warp.  The sums
+// stay in registers until the unit's end; its partial tile is then summed per
+// lag cell by ls_reduce in a fixed order.
 #include <algorithm>
 
 #include "lagspace.cuh"
@@ -24,7 +27,7 @@ namespace amber {
 namespace {
 
 constexpr int F_KX = 16;   // pixels per stage
-constexpr int F_NT = 256;  // threads per CTA
+constexpr int F_NT = 512;  // threads per CTA (16 warps: 4 along rows × 4 along columns)
 
 struct F64Desc {
     const double *m1, *m2, *m3;  // ring maps of r1, r2, r3 [nc][kp]
@@ -35,12 +38,18 @@ struct F64Desc {
     int nc, nc10, nclen, ks, AB;
 };
 
-// Shared-memory doubles of one stage for the largest staging the plan allows (row strides odd,
-// so that the transposed stores of 16 consecutive pixels hit 16 different bank pairs).
-constexpr int F_S1 = LS_ROWS * 2 + 1;  // D1 rows of an anchor block (AB ≤ 256 for k > 1)
-constexpr int F_S3 = LS_SPAN + 1;      // D3 span
-constexpr int F_S2 = LS_SPAN + 1;      // D2 span
-constexpr size_t F_SMEM = sizeof(double) * ((size_t)F_KX * (F_S1 + F_S3 + F_S2) + 2 * F_KX * LS_ROWS);
+constexpr int F_S1 = LS_SPAN + 1;  // D1 rows of an anchor block (≤ 256)
+constexpr int F_S3 = LS_SPAN + 1;  // D3 span
+constexpr int F_S2 = 260;          // D2 span (≤ 256), ≡ 4 mod 16
+constexpr int F_SA = 132;          // A buffer rows (128), ≡ 4 mod 16
+constexpr size_t F_SMEM = sizeof(double) * ((size_t)F_KX * (F_S1 + F_S3 + F_S2) + 2 * F_KX * F_SA);
+
+__device__ __forceinline__ void dmma(double &c0, double &c1, double a, double b)
+{
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(c0), "+d"(c1)
+                 : "d"(a), "d"(b));
+}
 
 __global__ void __launch_bounds__(F_NT, 1) ls_fp64_kernel(const F64Desc *__restrict__ jobs,
                                                           const LsUnit *__restrict__ units,
@@ -50,11 +59,13 @@ __global__ void __launch_bounds__(F_NT, 1) ls_fp64_kernel(const F64Desc *__restr
     double *st1 = sm;                    // [F_KX][F_S1]  w·D1 of the anchor block
     double *st3 = st1 + F_KX * F_S1;     // [F_KX][F_S3]  w·D3 of the span
     double *st2 = st3 + F_KX * F_S3;     // [F_KX][F_S2]  w·D2 of the span
-    double *As = st2 + F_KX * F_S2;      // [2][F_KX][LS_ROWS] the formed A operand
+    double *As = st2 + F_KX * F_S2;      // [2][F_KX][F_SA] the formed A operand
 
     const LsUnit u = units[blockIdx.x];
     const F64Desc j = jobs[u.job];
-    const int tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int wm = warp >> 2, wn = warp & 3;   // warp tile: rows 32·wm .., columns 32·wn ..
+    const int gq = lane >> 2, tq = lane & 3;   // fragment row / column group, k index
     const int ks = j.ks, nclen = j.nclen, nc = j.nc;
     const int c0 = u.ab * j.AB, c1 = min(nc, c0 + j.AB), nab1 = c1 - c0;
     const int mrows = ks > 1 ? ks * nclen : min(LS_ROWS, nclen - LS_ROWS * u.t3);
@@ -64,12 +75,16 @@ __global__ void __launch_bounds__(F_NT, 1) ls_fp64_kernel(const F64Desc *__restr
     const int span3 = nab1 + (ks > 1 ? nclen : mrows) - 1;
     const int span2 = nab1 + ncols - 1;
     const int g0 = j.group_off[u.ab], g1 = j.group_off[u.ab + 1];
+    // the A row this thread forms (pixels tid/128 + 4i), its anchor slot and lag
+    const int ar = tid & (LS_ROWS - 1), ax = tid >> 7;
+    const int aslot = ks > 1 ? ar / nclen : 0, ad3 = ks > 1 ? ar % nclen : ar;
+    const bool arow = ar < mrows;
 
-    double acc[8][8];
+    double acc[4][4][2];
 #pragma unroll
-    for (int i = 0; i < 8; ++i)
+    for (int mt = 0; mt < 4; ++mt)
 #pragma unroll
-        for (int q = 0; q < 8; ++q) acc[i][q] = 0.0;
+        for (int nt = 0; nt < 4; ++nt) acc[mt][nt][0] = acc[mt][nt][1] = 0.0;
 
     // stage rows [0, n) of map m starting at channel ch0, weighted, into st[x][row]
     auto stage = [&](double *st, int stride, const double *m, int ch0, int n, long x0) {
@@ -93,39 +108,38 @@ __global__ void __launch_bounds__(F_NT, 1) ls_fp64_kernel(const F64Desc *__restr
     for (long b = u.b0; b < u.b1; ++b) {
         const long xb = b * LS_BLOCK;
         for (long x0 = xb; x0 < min(j.k, xb + LS_BLOCK); x0 += F_KX) {
-            __syncthreads();  // the previous stage's readers are done
+            __syncthreads();  // every reader of the previous stage is done
             stage(st1, F_S1, j.m1, c0, nab1, x0);
             stage(st3, F_S3, j.m3, row0_3, span3, x0);
             stage(st2, F_S2, j.m2, row0_2, span2, x0);
+            __syncthreads();
             for (int g = g0; g < g1; ++g) {
                 const int pb = j.groups[g];
-                // A[x][r] = D1[p1, x] · D3[p1 − nc10 + Δ3, x] for slot a and lag Δ3 of row r
-                __syncthreads();  // stage visible; A[buf] no longer read by the group before last
-                double *A = As + buf * (F_KX * LS_ROWS);
-                for (int e = tid; e < F_KX * LS_ROWS; e += F_NT) {
-                    const int r = e % LS_ROWS, xx = e / LS_ROWS;
-                    double v = 0.0;
-                    if (r < mrows) {
-                        const int a = ks > 1 ? r / nclen : 0, d3 = ks > 1 ? r % nclen : r;
-                        const int p1 = pb + a;
-                        if (p1 < c1) v = st1[xx * F_S1 + (p1 - c0)] * st3[xx * F_S3 + (p1 - c0) + d3];
-                    }
-                    A[xx * LS_ROWS + r] = v;
+                // A[x][r] = D1[p1, x] · D3[p1 − nc10 + Δ3, x] for slot a and lag Δ3 of row r.  A[buf] was
+                // last read two groups ago, before the barrier that ended the previous formation.
+                double *A = As + buf * (F_KX * F_SA);
+                const int p1 = pb + aslot;
+                const bool ok = arow && p1 < c1;
+#pragma unroll
+                for (int i = 0; i < F_KX / 4; ++i) {
+                    const int xx = ax + 4 * i;
+                    A[xx * F_SA + ar] = ok ? st1[xx * F_S1 + (p1 - c0)] * st3[xx * F_S3 + (p1 - c0) + ad3] : 0.0;
                 }
                 __syncthreads();
-                const double *B = st2 + (pb - c0) + tx;  // column tx + 16q of the group's window
-#pragma unroll 4
-                for (int xx = 0; xx < F_KX; ++xx) {
-                    const double2 *ap = reinterpret_cast<const double2 *>(A + xx * LS_ROWS + ty * 8);
-                    const double2 a01 = ap[0], a23 = ap[1], a45 = ap[2], a67 = ap[3];
-                    const double av[8] = {a01.x, a01.y, a23.x, a23.y, a45.x, a45.y, a67.x, a67.y};
-                    double bv[8];
+                const double *Aw = A + 32 * wm + gq;
+                const double *Bw = st2 + (pb - c0) + 32 * wn + gq;
 #pragma unroll
-                    for (int q = 0; q < 8; ++q) bv[q] = B[xx * F_S2 + 16 * q];
+                for (int k4 = 0; k4 < F_KX / 4; ++k4) {
+                    const int xx = 4 * k4 + tq;
+                    double a[4], bv[4];
 #pragma unroll
-                    for (int i = 0; i < 8; ++i)
+                    for (int mt = 0; mt < 4; ++mt) a[mt] = Aw[xx * F_SA + 8 * mt];
 #pragma unroll
-                        for (int q = 0; q < 8; ++q) acc[i][q] = fma(av[i], bv[q], acc[i][q]);
+                    for (int nt = 0; nt < 4; ++nt) bv[nt] = Bw[xx * F_S2 + 8 * nt];
+#pragma unroll
+                    for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+                        for (int nt = 0; nt < 4; ++nt) dmma(acc[mt][nt][0], acc[mt][nt][1], a[mt], bv[nt]);
                 }
                 buf ^= 1;
             }
@@ -133,16 +147,19 @@ __global__ void __launch_bounds__(F_NT, 1) ls_fp64_kernel(const F64Desc *__restr
     }
     // the unit's partial tile [column][row]; slot a of a packed tile lands at lag column c − a
     double *out = partial + u.tile * (long)(LS_ROWS * LS_ROWS);
+    const int lagc = ks > 1 ? nclen : ncols;
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
-        const int r = ty * 8 + i;
+    for (int mt = 0; mt < 4; ++mt) {
+        const int r = 32 * wm + 8 * mt + gq;
         if (r >= mrows) continue;
         const int a = ks > 1 ? r / nclen : 0;
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            const int col = tx + 16 * q - a;
-            if (col >= 0 && col < (ks > 1 ? nclen : ncols)) out[(long)col * LS_ROWS + r] = acc[i][q];
-        }
+        for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int col = 32 * wn + 8 * nt + 2 * tq + h - a;
+                if (col >= 0 && col < lagc) out[(long)col * LS_ROWS + r] = acc[mt][nt][h];
+            }
     }
 }
 

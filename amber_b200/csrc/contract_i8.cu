@@ -51,6 +51,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <type_traits>
 #include <vector>
 
 #include "lagspace.cuh"
@@ -174,6 +175,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     uint64_t *acc_full = ab_empty + NABUF, *acc_empty = acc_full + 1, *drain = acc_empty + 1;
     volatile uint32_t *tmem_slot = reinterpret_cast<volatile uint32_t *>(drain + 1);
     volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
+    int *sgroups = reinterpret_cast<int *>(smem + NSTAGE * ST_BYTES + 256);  // this anchor block's groups
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const LsUnit u = units[blockIdx.x];
@@ -192,6 +194,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         return;
     }
 
+    for (int i = tid; i < g1 - g0; i += NTHREADS) sgroups[i] = jd->groups[g0 + i];
     if (tid == 0) {
         for (int s = 0; s < NSTAGE; ++s) { mbar_init(&st_full[s], 1); mbar_init(&st_empty[s], NFORM + 1); }
         for (int s = 0; s < NABUF; ++s) { mbar_init(&ab_full[s], NFORM); mbar_init(&ab_empty[s], 1); }
@@ -258,11 +261,11 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                         const int s = ns % NSTAGE;
                         if (!mbar_wait(&st_full[s], (ns / NSTAGE) & 1, abort_flag, err, 33)) { ok = false; break; }
                         const uint32_t d2base = smem_u32(smem + s * ST_BYTES + ST_D2);
-                        for (int g = g0; g < g1; ++g, ++na) {
+                        for (int g = 0; g < g1 - g0; ++g, ++na) {
                             const int ab = na % NABUF;
                             if (!mbar_wait(&ab_full[ab], (na / NABUF) & 1, abort_flag, err, 34)) { ok = false; break; }
                             fence_after();
-                            const uint32_t bw = d2base + (uint32_t)(jd->groups[g] - c0) * 16;  // window row 0
+                            const uint32_t bw = d2base + (uint32_t)(sgroups[g] - c0) * 16;  // window row 0
                             const uint32_t a0 = tmem + A_COL0 + ab * ABUF_COLS;
                             const uint32_t acc = fresh ? 0u : 1u;
                             if (sw == 0) {
@@ -298,67 +301,87 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         const int a = ks > 1 ? r / nclen : 0;             // anchor slot of the row
         const int d3 = ks > 1 ? r % nclen : r;            // lag Δ3 within the tile
         const bool row_ok = r < mrows;
+        const int row0_3 = c0 - jd->nc10 + (ks > 1 ? 0 : LS_ROWS * u.t3);  // channel of staged D3 row 0
         const uint32_t lane_field = (uint32_t)(32 * q) << 16;
+        const int ngr = g1 - g0, nab1 = c1 - c0;
         int ns = 0, na = 0, ni = 0;
+        // One iteration fills the A buffers of two anchor groups (one barrier round trip, one
+        // tcgen05.wait::st); lanes whose row has no data (past the tile, past the anchor block,
+        // or a D3 channel outside [0, nc)) store zero digits, and a warp with no such lane skips
+        // the arithmetic.
+        auto form_slice = [&](auto ndc, const unsigned char *st) {
+            constexpr int ND = decltype(ndc)::value;
+            for (int gi = 0; gi < ngr && ok; gi += 2) {
+                const int nb2 = min(2, ngr - gi);
+                for (int h = 0; h < nb2; ++h)
+                    if (!mbar_wait_warp(&ab_empty[(na + h) % NABUF], (((na + h) / NABUF) & 1) ^ 1, abort_flag, err,
+                                        36)) {
+                        ok = false;
+                        break;
+                    }
+                if (!ok) break;
+                uint32_t w[2][3][2];
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    if (h >= nb2) break;
+                    const int p1 = sgroups[gi + h] + a;
+                    const int rho = p1 - c0 + d3;  // staged D3 row of this lane
+                    const int p3 = row0_3 + rho;
+                    const bool valid = row_ok && p1 < c1 && p3 >= 0 && p3 < nc;
+#pragma unroll
+                    for (int dd = 0; dd < 3; ++dd) w[h][dd][0] = w[h][dd][1] = 0u;
+                    if (__any_sync(0xffffffffu, valid)) {
+                        const unsigned char *row3 = st + ST_D3 + min(rho, LS_SPAN - 1) * 128;
+                        const float4 x0 = *reinterpret_cast<const float4 *>(row3 + (((2 * ps) ^ (rho & 7)) << 4));
+                        const float4 x1 = *reinterpret_cast<const float4 *>(row3 + (((2 * ps + 1) ^ (rho & 7)) << 4));
+                        // the D1 row, already scaled by 127·2^−(E1+E3) for this block
+                        const float4 *row1 =
+                            reinterpret_cast<const float4 *>(st + ST_D1 + min(p1 - c0, nab1 - 1) * 128 + 32 * ps);
+                        const float4 u0 = row1[0], u1 = row1[1];
+                        float2 ya[4], yb[4], yc[4], yd[4];
+                        digits254x2<ND>(make_float2(u0.x, u0.y), make_float2(x0.x, x0.y), ya);
+                        digits254x2<ND>(make_float2(u0.z, u0.w), make_float2(x0.z, x0.w), yb);
+                        digits254x2<ND>(make_float2(u1.x, u1.y), make_float2(x1.x, x1.y), yc);
+                        digits254x2<ND>(make_float2(u1.z, u1.w), make_float2(x1.z, x1.w), yd);
+                        constexpr int D0 = ND - 3;  // sweep 2 stores product digits 1-3
+#pragma unroll
+                        for (int dd = 0; dd < 3; ++dd) {
+                            w[h][dd][0] = valid ? pack_low_bytes(ya[dd + D0].x, ya[dd + D0].y, yb[dd + D0].x,
+                                                                 yb[dd + D0].y)
+                                                : 0u;
+                            w[h][dd][1] = valid ? pack_low_bytes(yc[dd + D0].x, yc[dd + D0].y, yd[dd + D0].x,
+                                                                 yd[dd + D0].y)
+                                                : 0u;
+                        }
+                    }
+                    // pixels 8ps .. 8ps+7 of the slice = columns 2ps, 2ps+1 of each digit's 8
+                    const uint32_t col = tmem + lane_field + A_COL0 + ((na + h) % NABUF) * ABUF_COLS + 2 * ps;
+#pragma unroll
+                    for (int dd = 0; dd < 3; ++dd) tmem_st2(col + 8 * dd, w[h][dd][0], w[h][dd][1]);
+                }
+                // tcgen05.st reads its source registers asynchronously: wait before they change
+                asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+                fence_before();
+                __syncwarp();
+                if (lane == 0)
+                    for (int h = 0; h < nb2; ++h) mbar_arrive(&ab_full[(na + h) % NABUF]);
+                na += nb2;
+            }
+        };
         for (long b = u.b0; b < u.b1 && ok; ++b) {
             const int E13 = jd->e1[b] + jd->e3[b];
             const float sc = ldexpf(127.f, -E13);
-            const float2 sc2 = make_float2(sc, sc);
             for (int sw = 0; sw < sweeps && ok; ++sw, ++ni) {
                 for (int sl = 0; sl < nslices(b) && ok; ++sl, ++ns) {
                     const int s = ns % NSTAGE;
                     if (!mbar_wait_warp(&st_full[s], (ns / NSTAGE) & 1, abort_flag, err, 35)) { ok = false; break; }
-                    const unsigned char *st = smem + s * ST_BYTES;
-                    for (int g = g0; g < g1; ++g, ++na) {
-                        const int ab = na % NABUF;
-                        if (!mbar_wait_warp(&ab_empty[ab], ((na / NABUF) & 1) ^ 1, abort_flag, err, 36)) {
-                            ok = false;
-                            break;
-                        }
-                        const int p1 = jd->groups[g] + a;
-                        uint32_t w[3][2] = {{0u, 0u}, {0u, 0u}, {0u, 0u}};
-                        if (row_ok && p1 < c1) {
-                            const int rho = p1 - c0 + d3;  // staged D3 row of this lane
-                            const unsigned char *row3 = st + ST_D3 + rho * 128;
-                            const float4 x0 = *reinterpret_cast<const float4 *>(row3 + (((2 * ps) ^ (rho & 7)) << 4));
-                            const float4 x1 =
-                                *reinterpret_cast<const float4 *>(row3 + (((2 * ps + 1) ^ (rho & 7)) << 4));
-                            const float4 *row1 =
-                                reinterpret_cast<const float4 *>(st + ST_D1 + (p1 - c0) * 128 + 32 * ps);
-                            const float4 u0 = row1[0], u1 = row1[1];
-                            float2 ya[4], yb[4], yc[4], yd[4];
-                            if (sw == 0) {
-                                digits254x2<3>(__fmul2_rn(make_float2(u0.x, u0.y), sc2), make_float2(x0.x, x0.y), ya);
-                                digits254x2<3>(__fmul2_rn(make_float2(u0.z, u0.w), sc2), make_float2(x0.z, x0.w), yb);
-                                digits254x2<3>(__fmul2_rn(make_float2(u1.x, u1.y), sc2), make_float2(x1.x, x1.y), yc);
-                                digits254x2<3>(__fmul2_rn(make_float2(u1.z, u1.w), sc2), make_float2(x1.z, x1.w), yd);
-#pragma unroll
-                                for (int dd = 0; dd < 3; ++dd) {
-                                    w[dd][0] = pack_low_bytes(ya[dd].x, ya[dd].y, yb[dd].x, yb[dd].y);
-                                    w[dd][1] = pack_low_bytes(yc[dd].x, yc[dd].y, yd[dd].x, yd[dd].y);
-                                }
-                            } else {
-                                digits254x2<4>(__fmul2_rn(make_float2(u0.x, u0.y), sc2), make_float2(x0.x, x0.y), ya);
-                                digits254x2<4>(__fmul2_rn(make_float2(u0.z, u0.w), sc2), make_float2(x0.z, x0.w), yb);
-                                digits254x2<4>(__fmul2_rn(make_float2(u1.x, u1.y), sc2), make_float2(x1.x, x1.y), yc);
-                                digits254x2<4>(__fmul2_rn(make_float2(u1.z, u1.w), sc2), make_float2(x1.z, x1.w), yd);
-#pragma unroll
-                                for (int dd = 0; dd < 3; ++dd) {
-                                    w[dd][0] = pack_low_bytes(ya[dd + 1].x, ya[dd + 1].y, yb[dd + 1].x, yb[dd + 1].y);
-                                    w[dd][1] = pack_low_bytes(yc[dd + 1].x, yc[dd + 1].y, yd[dd + 1].x, yd[dd + 1].y);
-                                }
-                            }
-                        }
-                        // pixels 8ps .. 8ps+7 of the slice = columns 2ps, 2ps+1 of each digit's 8
-                        const uint32_t col = tmem + lane_field + A_COL0 + ab * ABUF_COLS + 2 * ps;
-#pragma unroll
-                        for (int dd = 0; dd < 3; ++dd) tmem_st2(col + 8 * dd, w[dd][0], w[dd][1]);
-                        // tcgen05.st reads its source registers asynchronously: wait before they change
-                        asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
-                        fence_before();
-                        __syncwarp();
-                        if (lane == 0) mbar_arrive(&ab_full[ab]);
-                    }
+                    unsigned char *st = smem + s * ST_BYTES;
+                    // scale the staged D1 rows once for every row that uses them (the formers alone read them)
+                    float *d1 = reinterpret_cast<float *>(st + ST_D1);
+                    for (int e = tid; e < nab1 * SLICE; e += NFORM * 32) d1[e] *= sc;
+                    asm volatile("bar.sync 1, %0;" ::"n"(NFORM * 32) : "memory");
+                    if (sw == 0) form_slice(std::integral_constant<int, 3>(), st);
+                    else form_slice(std::integral_constant<int, 4>(), st);
                     __syncwarp();
                     if (ok && lane == 0) mbar_arrive(&st_empty[s]);
                 }
@@ -406,7 +429,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     }
 }
 
-constexpr size_t SMEM_BYTES = 1024 + (size_t)NSTAGE * ST_BYTES + 256;
+constexpr size_t SMEM_BYTES = 1024 + (size_t)NSTAGE * ST_BYTES + 256 + sizeof(int) * LS_SPAN;
 
 typedef CUresult (*EncodeTiled)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
                                 const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,

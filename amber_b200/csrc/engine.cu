@@ -58,6 +58,7 @@ struct Request {
     int nc10 = 0;
     std::vector<int> uf;
     int want_v2 = 0;
+    const double *d_re_im = nullptr, *d_ntig = nullptr;  // caller-owned device cube (read in place)
     bool want_cyl = false;  // cylindrical bispectra of every triangle as well
     amber_cuda_cylbs_params cyl{};
     // plan
@@ -104,7 +105,7 @@ size_t footprint_of(const Request &r, int precision, long nslots_max)
 {
     const size_t cells = (size_t)r.N1 * (size_t)(r.N1 / 2 + 1);
     const size_t grid = sizeof(double) * 3 * cells * r.nc;         // double2 grid + double mask
-    const size_t staging = sizeof(double) * 3 * cells * r.nc;      // raw sums + counts on upload
+    const size_t staging = r.d_re_im ? 0 : sizeof(double) * 3 * cells * r.nc;  // raw sums + counts on upload
     const size_t Nr = r.ulow.size();
     const size_t calcr_maps = sizeof(double) * Nr * (size_t)r.N1 * r.N1;
     const int nclen = 2 * r.nc10 + 1;
@@ -173,7 +174,9 @@ int Engine::setup(Request *r)
     if (rc) return rc;
     amber_cuda_ctx *s = r->sub;
     s->contracts_elsewhere = owner->precision == AMBER_PREC_MIXED;
-    if ((rc = amber_cuda_load_grid_packed(s, r->N1, r->nc, r->Du, r->flag_key, r->re_im.data(), r->ntig.data())))
+    if ((rc = r->d_re_im ? amber_cuda_load_grid_device(s, r->N1, r->nc, r->Du, r->flag_key, r->d_re_im, r->d_ntig)
+                         : amber_cuda_load_grid_packed(s, r->N1, r->nc, r->Du, r->flag_key, r->re_im.data(),
+                                                       r->ntig.data())))
         return rc;
     // the host copies are no longer needed once the cube is on the device
     std::vector<double>().swap(r->re_im);
@@ -287,7 +290,7 @@ void Engine::loop()
         const double t0 = now_ms();
         // this round's share of the statistics, published under the lock at its end
         double setup_ms = 0, maps_ms = 0, contract_ms = 0, finish_ms = 0;
-        long launches = 0;
+        long launches = 0, all_launches = 0;
         owner->phase_used = 0;  // per-phase timing events are reused round after round
         // one map-set batch of every active request
         std::vector<I8Job> jobs;
@@ -295,7 +298,10 @@ void Engine::loop()
         for (Request *r : round) {
             int rc = AMBER_OK;
             double ta = now_ms();
-            if (!r->started) rc = setup(r);
+            if (!r->started) {
+                rc = setup(r);
+                if (r->sub) all_launches += r->sub->launches;  // grid normalisation and calCR of the new request
+            }
             setup_ms += now_ms() - ta;
             if (!rc && run_finished(r->run)) {
                 finish(r);  // no triangles at all
@@ -303,7 +309,9 @@ void Engine::loop()
             }
             if (!rc) {
                 ta = now_ms();
+                const long launched = r->sub->launches;
                 rc = run_next_batch(r->sub, r->run, &jobs);
+                all_launches += r->sub->launches - launched;
                 rc = rc < 0 ? rc : AMBER_OK;
                 maps_ms += now_ms() - ta;
             }
@@ -315,10 +323,19 @@ void Engine::loop()
         }
         int rc = AMBER_OK;
         double tc = now_ms();
+        double kernel_ms = 0;
         if (!jobs.empty()) {
-            const long before = owner->contractions;
-            rc = contract_i8_jobs(owner, jobs);
+            const long before = owner->contractions, launched = owner->launches;
+            rc = contract_i8_jobs(owner, jobs);  // synchronises the stream
             launches = owner->contractions - before;
+            all_launches += owner->launches - launched;
+            for (size_t i = 0; i < owner->phase_used; ++i)
+                if (owner->phase_ev[i].phase == 1) {
+                    float ms = 0;
+                    if (cudaEventElapsedTime(&ms, owner->phase_ev[i].a, owner->phase_ev[i].b) == cudaSuccess)
+                        kernel_ms += ms;
+                }
+            cudaGetLastError();
         }
         contract_ms = now_ms() - tc;
         tc = now_ms();
@@ -336,6 +353,8 @@ void Engine::loop()
         info.contract_ms += contract_ms;
         info.finish_ms += finish_ms;
         info.contraction_launches += launches;
+        info.kernel_launches += all_launches;
+        info.contract_kernel_ms += kernel_ms;
         info.rounds += 1;
         info.busy_ms += now_ms() - t0;
     }
@@ -402,8 +421,13 @@ int amber_cuda_enqueue(amber_cuda_ctx *c, const amber_cuda_request *q, int64_t *
     r->Du = q->Du;
     r->flag_key = q->flag_key;
     const size_t cells = (size_t)q->N1 * (size_t)(q->N1 / 2 + 1);
-    r->re_im.assign(q->re_im, q->re_im + 2 * cells * q->nc);
-    r->ntig.assign(q->ntig, q->ntig + cells * q->nc);
+    if (q->inputs_on_device) {
+        r->d_re_im = q->re_im;
+        r->d_ntig = q->ntig;
+    } else {
+        r->re_im.assign(q->re_im, q->re_im + 2 * cells * q->nc);
+        r->ntig.assign(q->ntig, q->ntig + cells * q->nc);
+    }
     r->ulow.assign(q->ULow, q->ULow + q->Nr);
     r->uhigh.assign(q->UHigh, q->UHigh + q->Nr);
     r->nc10 = q->nc10;

@@ -76,6 +76,10 @@ AMBER_API int amber_cuda_load_grid_packed(amber_cuda_ctx *ctx, long N1, long nc,
                                 const double *re_im, const double *ntig);
 AMBER_API int amber_cuda_load_grid(amber_cuda_ctx *ctx, long N1, long nc, double Du, int flag_key,
                          const double *const *GVre, const double *const *GVim, const double *const *NTiG);
+/* The packed form with re_im and ntig already in device memory on the context's device (a cube
+ * kept resident between estimates): normalised straight from there, nothing is copied in. */
+AMBER_API int amber_cuda_load_grid_device(amber_cuda_ctx *ctx, long N1, long nc, double Du, int flag_key,
+                                          const double *re_im, const double *ntig);
 
 /* ---- ring edges: replaces annular_rings (amber_funcs.c:2022-2094).  Uavg is
  * computed as in amber_funcs.c:2065.  Rings must lie inside the grid
@@ -257,6 +261,9 @@ typedef struct amber_cuda_request {
     const int *uf_chans;
     int want_v2;
     const amber_cuda_cylbs_params *cylbs; /* NULL, or: also the cylindrical bispectra (copied on enqueue) */
+    int inputs_on_device; /* 1: re_im and ntig are device pointers on the context's device, read in place
+                             when the request is admitted (keep them unchanged until it is done); 0: host
+                             memory, copied on enqueue */
 } amber_cuda_request;
 
 typedef struct amber_cuda_engine_info {
@@ -273,6 +280,8 @@ typedef struct amber_cuda_engine_info {
     double maps_ms;            /*   ring-map batches */
     double contract_ms;        /*   contractions and lag reductions */
     double finish_ms;          /*   results back to the host, child contexts freed */
+    long kernel_launches;      /* library kernels launched by the rounds (maps, contractions, reductions) */
+    double contract_kernel_ms; /* device time of the contraction kernels (CUDA events on the launch stream) */
 } amber_cuda_engine_info;
 
 AMBER_API int amber_cuda_enqueue(amber_cuda_ctx *ctx, const amber_cuda_request *req, int64_t *ticket);

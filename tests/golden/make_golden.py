@@ -14,7 +14,10 @@ outputs as compressed .npz files:
                      cl_dnu computes from it (oracle/_ref/ref_maps);
   cylbs_ref.npz    — seeded lag arrays and the cylindrical bispectra that the
                      reference's analysis Python (mabs_funcs.get_cyl_BS,
-                     mfunc_winds.cylbs_win) computes from them.
+                     mfunc_winds.cylbs_win) computes from them;
+  c2_rp217_ref64.npz — one Ng1 = 740 triangle of the single-realisation
+                     workload at full size, v1 and v2, from the FP64 build
+                     (outputs only; the inputs are regenerated from their seed).
 
 Needs the reference sources (make -C oracle ref); run from the repo root:
     python tests/golden/make_golden.py
@@ -72,6 +75,27 @@ def est_case(name, nn, nc, seed, nbins, hi, nc10, flagged):
                total_vcp=st64["total_vcp"])
     np.savez_compressed(os.path.join(OUT, f"est_{name}.npz"), **rec)
     print(name, "triangles", len(rdata), "total_vcp", st64["total_vcp"])
+
+
+def c2_full_case(rp=217):
+    """One Ng1 = 740 triangle of the single-realisation workload (256² grid, 128 channels with the
+    block-edge flags, 16 bins, nc10 = 63) at full size, through the reference's FP64 build, v1 and
+    v2.  Only outputs are stored: the inputs are regenerated by synth.config2(seed=1) (seeded), and
+    a SHA-256 of the grid and the counts guards against the generator drifting."""
+    import hashlib
+    real = synth.config2(seed=1)
+    nclen = real.nclen
+    st1, rp1 = oracle.run_ref_amber(real, oracle.tmpdir(), version=1, fp64=True, rp_begin=rp, rp_end=rp + 1)
+    st2, rp2 = oracle.run_ref_amber(real, oracle.tmpdir(), version=2, fp64=True, rp_begin=rp, rp_end=rp + 1)
+    rdata = formats.read_closed_rings(rp1)
+    r1, r2, r3 = (int(v) for v in rdata[rp, :3])
+    t, nu, bl, nd = formats.read_bsout_v1(os.path.join(rp1, formats.bsout_name(1, r1, r2, r3, 1)), nclen, np.float64)
+    iv, blv, ndv = formats.read_bsout_v2(os.path.join(rp2, formats.bsout_name(2, r1, r2, r3, 1)), nclen, np.float64)
+    h = hashlib.sha256(np.ascontiguousarray(real.gv).tobytes() + np.ascontiguousarray(real.counts).tobytes())
+    np.savez_compressed(os.path.join(OUT, f"c2_rp{rp}_ref64.npz"), rp=rp, tri=np.array([r1, r2, r3]),
+                        rdata_num=rdata[rp, 3], ntri=t, num=nu, bldnu64=bl, numdnu=nd, bldnu_v2=blv, numtri_v2=ndv,
+                        inv_ng=iv, total_vcp=st1["total_vcp"], inputs_sha256=h.hexdigest())
+    print("c2 rp", rp, (r1, r2, r3), "total_vcp", st1["total_vcp"], "v1", st1["accum_s"], "s, v2", st2["accum_s"], "s")
 
 
 GRID_CASES = {
@@ -156,3 +180,4 @@ if __name__ == "__main__":
         grid_case(k, *v, collapse=True)
     cylbs_case()
     maps_case()
+    c2_full_case()  # ~10 min on 8 host threads

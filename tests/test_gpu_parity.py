@@ -327,3 +327,81 @@ def test_error_paths(lib_built):
         # still usable after errors
         rd = est.calcr()
         assert len(rd) > 0
+
+
+C2_FIXTURE = os.path.join(GOLDEN, "c2_rp217_ref64.npz")
+
+
+@pytest.mark.skipif(not os.path.exists(C2_FIXTURE), reason="full-size fixture not generated")
+def test_config2_full_size_triangle_vs_reference_build(lib_built):
+    """One Ng1 = 740 triangle (rp = 217) of the single-realisation workload at full size — 256² grid,
+    128 channels with the block-edge flags, nc10 = 63, 810152 channel triplets × 547600 pixels —
+    against the reference's own FP64 build (tests/golden/c2_rp217_ref64.npz, v1 and v2 files).
+    FP64 path within 1e-10 and the mixed path within 1e-6 of Σ|products| per lag cell (the FP64
+    path on |maps| gives that scale); counts and the file scalars exact."""
+    import hashlib
+    import amber_b200
+    z = np.load(C2_FIXTURE)
+    real = synth.config2(seed=1)
+    h = hashlib.sha256(np.ascontiguousarray(real.gv).tobytes() + np.ascontiguousarray(real.counts).tobytes())
+    assert h.hexdigest() == str(z["inputs_sha256"]), "the seeded generator no longer makes the fixture's inputs"
+    rp = int(z["rp"])
+    out = {}
+    for prec in ("fp64", "mixed", "fp64_abs"):
+        with amber_b200.Estimator(precision=prec) as est:
+            est.load_grid(real.gv, real.counts, real.du, real.flag_key)
+            est.set_rings(real.ulow, real.uhigh)
+            est.set_channels(real.nc10, real.uf_chans)
+            rd = est.calcr()
+            tri = rd[[rp], :3].astype(np.int32)
+            assert np.array_equal(tri[0], z["tri"])
+            bl, nd, nt = est.triangles(tri, want_v2=True)
+            out[prec] = (bl[0].reshape(real.nclen, real.nclen), nd[0].reshape(real.nclen, real.nclen),
+                         nt[0].reshape(real.nclen, real.nclen))
+            if prec == "fp64":
+                r1, r2, r3 = (int(v) for v in z["tri"])
+                ntri, num, _, n1 = est.triangle_v1(r1, r2, r3, float(rd[rp, 3]))
+                assert np.array_equal(n1, z["numdnu"])
+                np.testing.assert_allclose([ntri, num], [float(z["ntri"]), float(z["num"])], rtol=1e-12)
+    ab_bl, _, ab_nt = out["fp64_abs"]
+    for prec, tol in (("fp64", 1e-10), ("mixed", 1e-6)):
+        bl, nd, nt = out[prec]
+        np.testing.assert_array_equal(nd, z["numdnu"])
+        for ours, ref, scale in ((bl, z["bldnu64"], ab_bl), (bl, z["bldnu_v2"], ab_bl), (nt, z["numtri_v2"], ab_nt)):
+            e = np.abs(ours - ref) / (scale + 1e-300)
+            assert e.max() <= tol, (prec, e.max())
+
+
+def _first_with_ng(real, ng_min):
+    tri = oracle.triangles(real.ulow, real.uhigh)
+    for i, t in enumerate(tri):
+        if oracle.ng1(real.uhigh[int(t[0])], real.du) >= ng_min:
+            return i
+    return len(tri) - 1
+
+
+@pytest.mark.parametrize("side", [96, 128, 192, 256, 320])
+def test_ensemble_realisation_at_real_size_vs_oracle(side, lib_built):
+    """The first realisation of each grid side in the 64-realisation ensemble, at its real size
+    (its grid, channel count, flags and 12 rings), through the request engine; two of its triangles
+    (the smallest map and the first with Ng1 ≥ 70) against the FP64 oracle.  Side 128 has
+    nclen = 131, so its lag window spans 2 × 2 tiles."""
+    import amber_b200
+    specs = synth.config3_specs()
+    spec = next(s for s in specs if s["nn"] == side)
+    real = synth.from_spec(spec)
+    pick = [0, _first_with_ng(real, 70)]
+    with amber_b200.Estimator(precision="mixed") as est:
+        eng = amber_b200.Engine(est)
+        t = eng.enqueue(real, want_v2=True)
+        rd, bl, nd, nt, _ = eng.result(t, real, want_v2=True)
+    ordata, ores = oracle.estimate(real, version=2, tri_subset=pick, with_absscale=True)
+    np.testing.assert_array_equal(rd[:, :3], ordata[:, :3])
+    n = real.nclen
+    for o in ores:
+        i = o["rp"]
+        np.testing.assert_array_equal(nd[i].reshape(n, n), o["numdnu"])
+        e = np.abs(bl[i].reshape(n, n) - o["bldnu"]) / (o["absscale"] + 1e-300)
+        assert e.max() <= 1e-6, (side, i, e.max())
+        ei = np.abs(nt[i].reshape(n, n) - o["numtri"]) / (o["absscale_i"] + 1e-300)
+        assert ei.max() <= 1e-6, (side, i, ei.max())
