@@ -6,13 +6,13 @@
 // The contraction is the lag-space GEMM of lagspace.cuh: per unit (a tile pair,
 // an anchor block and a run of pixel blocks) one CTA of 8 warps holds a 128 × 128
 // FP64 accumulator tile in registers, 16 warps each holding a 32 × 32 block as
-// 4 × 4 fragments of the FP64 tensor-core MMA (mma.sync m8n8k4); four warps per
-// SM sub-partition keep its FP64 pipe fed.  Per stage of 16
+// 2 × 4 fragments of the FP64 tensor-core MMA mma.sync m16n8k8 (1024 FMAs per
+// instruction; the m8n8k4 shape reaches only about half the FP64 tensor rate).  Per stage of 16
 // pixels the CTA copies the channel rows its anchors touch — w·D1 of the anchor
 // block, w·D3 and w·D2 of the spans their windows cover — into shared memory
 // once (transposed, [pixel][channel]); then, for every anchor group, it forms
 // the A operand D1[p1]·D3[p1 − nc10 + Δ3] (one multiply per element, into one
-// of two buffers) and runs four k = 4 steps of 16 MMAs per warp, reading B
+// of two buffers) and runs two k = 8 steps of 8 MMAs per warp, reading B
 // straight from the staged D2 rows at the group's window offset.  Row strides
 // of the A buffer and the D2 stage are ≡ 4 (mod 16) doubles, so a fragment
 // load (4 pixels × 8 rows) hits 16 distinct bank pairs per half warp.  The sums
@@ -44,11 +44,14 @@ constexpr int F_S2 = 260;          // D2 span (≤ 256), ≡ 4 mod 16
 constexpr int F_SA = 132;          // A buffer rows (128), ≡ 4 mod 16
 constexpr size_t F_SMEM = sizeof(double) * ((size_t)F_KX * (F_S1 + F_S3 + F_S2) + 2 * F_KX * F_SA);
 
-__device__ __forceinline__ void dmma(double &c0, double &c1, double a, double b)
+// D(16×8) += A(16×8) · B(8×8), FP64.  Fragments (g = lane / 4, t = lane % 4): A {(g, t), (g+8, t),
+// (g, t+4), (g+8, t+4)}, B {(t, g), (t+4, g)}, C {(g, 2t), (g, 2t+1), (g+8, 2t), (g+8, 2t+1)}.
+__device__ __forceinline__ void dmma(double (&c)[4], const double (&a)[4], const double (&b)[2])
 {
-    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
-                 : "+d"(c0), "+d"(c1)
-                 : "d"(a), "d"(b));
+    asm volatile("mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+                 "{%0, %1, %2, %3};"
+                 : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+                 : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
 }
 
 __global__ void __launch_bounds__(F_NT, 1) ls_fp64_kernel(const F64Desc *__restrict__ jobs,
@@ -80,11 +83,13 @@ __global__ void __launch_bounds__(F_NT, 1) ls_fp64_kernel(const F64Desc *__restr
     const int aslot = ks > 1 ? ar / nclen : 0, ad3 = ks > 1 ? ar % nclen : ar;
     const bool arow = ar < mrows;
 
-    double acc[4][4][2];
+    double acc[2][4][4];
 #pragma unroll
-    for (int mt = 0; mt < 4; ++mt)
+    for (int mt = 0; mt < 2; ++mt)
 #pragma unroll
-        for (int nt = 0; nt < 4; ++nt) acc[mt][nt][0] = acc[mt][nt][1] = 0.0;
+        for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) acc[mt][nt][e] = 0.0;
 
     // stage rows [0, n) of map m starting at channel ch0, weighted, into st[x][row]
     auto stage = [&](double *st, int stride, const double *m, int ch0, int n, long x0) {
@@ -129,17 +134,25 @@ __global__ void __launch_bounds__(F_NT, 1) ls_fp64_kernel(const F64Desc *__restr
                 const double *Aw = A + 32 * wm + gq;
                 const double *Bw = st2 + (pb - c0) + 32 * wn + gq;
 #pragma unroll
-                for (int k4 = 0; k4 < F_KX / 4; ++k4) {
-                    const int xx = 4 * k4 + tq;
-                    double a[4], bv[4];
+                for (int k8 = 0; k8 < F_KX / 8; ++k8) {
+                    const int xx = 8 * k8 + tq;
+                    double a[2][4], bv[4][2];
 #pragma unroll
-                    for (int mt = 0; mt < 4; ++mt) a[mt] = Aw[xx * F_SA + 8 * mt];
+                    for (int mt = 0; mt < 2; ++mt) {
+                        a[mt][0] = Aw[xx * F_SA + 16 * mt];
+                        a[mt][1] = Aw[xx * F_SA + 16 * mt + 8];
+                        a[mt][2] = Aw[(xx + 4) * F_SA + 16 * mt];
+                        a[mt][3] = Aw[(xx + 4) * F_SA + 16 * mt + 8];
+                    }
 #pragma unroll
-                    for (int nt = 0; nt < 4; ++nt) bv[nt] = Bw[xx * F_S2 + 8 * nt];
+                    for (int nt = 0; nt < 4; ++nt) {
+                        bv[nt][0] = Bw[xx * F_S2 + 8 * nt];
+                        bv[nt][1] = Bw[(xx + 4) * F_S2 + 8 * nt];
+                    }
 #pragma unroll
-                    for (int mt = 0; mt < 4; ++mt)
+                    for (int mt = 0; mt < 2; ++mt)
 #pragma unroll
-                        for (int nt = 0; nt < 4; ++nt) dmma(acc[mt][nt][0], acc[mt][nt][1], a[mt], bv[nt]);
+                        for (int nt = 0; nt < 4; ++nt) dmma(acc[mt][nt], a[mt], bv[nt]);
                 }
                 buf ^= 1;
             }
@@ -149,18 +162,20 @@ __global__ void __launch_bounds__(F_NT, 1) ls_fp64_kernel(const F64Desc *__restr
     double *out = partial + u.tile * (long)(LS_ROWS * LS_ROWS);
     const int lagc = ks > 1 ? nclen : ncols;
 #pragma unroll
-    for (int mt = 0; mt < 4; ++mt) {
-        const int r = 32 * wm + 8 * mt + gq;
-        if (r >= mrows) continue;
-        const int a = ks > 1 ? r / nclen : 0;
+    for (int mt = 0; mt < 2; ++mt)
 #pragma unroll
-        for (int nt = 0; nt < 4; ++nt)
+        for (int hr = 0; hr < 2; ++hr) {
+            const int r = 32 * wm + 16 * mt + 8 * hr + gq;
+            if (r >= mrows) continue;
+            const int a = ks > 1 ? r / nclen : 0;
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int col = 32 * wn + 8 * nt + 2 * tq + h - a;
-                if (col >= 0 && col < lagc) out[(long)col * LS_ROWS + r] = acc[mt][nt][h];
-            }
-    }
+            for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int col = 32 * wn + 8 * nt + 2 * tq + h - a;
+                    if (col >= 0 && col < lagc) out[(long)col * LS_ROWS + r] = acc[mt][nt][2 * hr + h];
+                }
+        }
 }
 
 // Pass 1 of the lag reduction: unit group g of cell d sums partial[u][d] for

@@ -151,6 +151,32 @@ __device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, u
         : "memory");
 }
 
+// kind::i8 MMA, A from TMEM, issued by the lane elect.sync picks from the converged MMA warp (every
+// operand is warp-uniform, so the issue costs one instruction), with the accumulate operand as an
+// immediate: the first MMA into an accumulator overwrites it, the rest add.
+__device__ __forceinline__ void umma_i8_set(uint32_t d_tmem, uint32_t a_tmem, uint64_t b_desc, uint32_t idesc)
+{
+    asm volatile("{\n\t.reg .pred e;\n\telect.sync _|e, 0xffffffff;\n\t"
+                 "@e tcgen05.mma.cta_group::1.kind::i8 [%0], [%1], %2, %3, 0;\n\t}" ::"r"(d_tmem), "r"(a_tmem),
+                 "l"(b_desc), "r"(idesc)
+                 : "memory");
+}
+__device__ __forceinline__ void umma_i8_add(uint32_t d_tmem, uint32_t a_tmem, uint64_t b_desc, uint32_t idesc)
+{
+    asm volatile("{\n\t.reg .pred e;\n\telect.sync _|e, 0xffffffff;\n\t"
+                 "@e tcgen05.mma.cta_group::1.kind::i8 [%0], [%1], %2, %3, 1;\n\t}" ::"r"(d_tmem), "r"(a_tmem),
+                 "l"(b_desc), "r"(idesc)
+                 : "memory");
+}
+// tcgen05.commit from the elected lane of the converged warp
+__device__ __forceinline__ void umma_commit_elect(uint64_t *bar)
+{
+    asm volatile("{\n\t.reg .pred e;\n\telect.sync _|e, 0xffffffff;\n\t"
+                 "@e tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n\t}" ::"r"(
+                     smem_u32(bar))
+                 : "memory");
+}
+
 // Shared-memory descriptor of a K-major operand without swizzle: 8-row core matrices of
 // 16-byte rows stacked every 128 bytes (SBO), the second 16-byte K chunk `lbo` bytes on.
 __device__ __forceinline__ uint64_t smem_desc_plain(uint32_t saddr, uint32_t lbo)
@@ -176,6 +202,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     volatile uint32_t *tmem_slot = reinterpret_cast<volatile uint32_t *>(drain + 1);
     volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
     int *sgroups = reinterpret_cast<int *>(smem + NSTAGE * ST_BYTES + 256);  // this anchor block's groups
+    unsigned char *zero_row = smem + NSTAGE * ST_BYTES + 256 + sizeof(int) * LS_SPAN;  // 128 zero bytes
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const LsUnit u = units[blockIdx.x];
@@ -195,6 +222,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     }
 
     for (int i = tid; i < g1 - g0; i += NTHREADS) sgroups[i] = jd->groups[g0 + i];
+    if (tid < 32) reinterpret_cast<uint32_t *>(zero_row)[tid] = 0u;
     if (tid == 0) {
         for (int s = 0; s < NSTAGE; ++s) { mbar_init(&st_full[s], 1); mbar_init(&st_empty[s], NFORM + 1); }
         for (int s = 0; s < NABUF; ++s) { mbar_init(&ab_full[s], NFORM); mbar_init(&ab_empty[s], 1); }
@@ -245,54 +273,66 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                         __nanosleep(100);
         }
     } else if (warp == WARP_MMA) {
-        if (lane == 0) {
-            // S32 accumulate, signed int8 A and B, both K-major, M = 128, N = nmma
-            const uint32_t idesc = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(nmma >> 3) << 17) |
-                                   ((uint32_t)(LS_ROWS >> 4) << 24);
-            const uint32_t lbo = (uint32_t)jd->span2 * 16;   // the second 16-pixel group of a digit
-            const uint32_t dstride = 2 * lbo;                // the next digit
-            int ns = 0, na = 0, ni = 0;
-            for (long b = u.b0; b < u.b1 && ok; ++b)
-                for (int sw = 0; sw < sweeps && ok; ++sw, ++ni) {
-                    // the epilogue of the previous item has read the accumulators out
-                    if (!mbar_wait(acc_empty, (ni & 1) ^ 1, abort_flag, err, 32)) { ok = false; break; }
-                    bool fresh = true;
-                    for (int sl = 0; sl < nslices(b) && ok; ++sl, ++ns) {
-                        const int s = ns % NSTAGE;
-                        if (!mbar_wait(&st_full[s], (ns / NSTAGE) & 1, abort_flag, err, 33)) { ok = false; break; }
-                        const uint32_t d2base = smem_u32(smem + s * ST_BYTES + ST_D2);
-                        for (int g = 0; g < g1 - g0; ++g, ++na) {
-                            const int ab = na % NABUF;
-                            if (!mbar_wait(&ab_full[ab], (na / NABUF) & 1, abort_flag, err, 34)) { ok = false; break; }
-                            fence_after();
-                            const uint32_t bw = d2base + (uint32_t)(sgroups[g] - c0) * 16;  // window row 0
-                            const uint32_t a0 = tmem + A_COL0 + ab * ABUF_COLS;
-                            const uint32_t acc = fresh ? 0u : 1u;
-                            if (sw == 0) {
-                                // class k = Σ_{i+j=k} Q_i·P_j into accumulator k
-                                umma_ts_i8(tmem, a0, smem_desc_plain(bw, lbo), idesc, acc);
-                                umma_ts_i8(tmem + ACC_STRIDE, a0 + 8, smem_desc_plain(bw, lbo), idesc, acc);
-                                umma_ts_i8(tmem + ACC_STRIDE, a0, smem_desc_plain(bw + dstride, lbo), idesc, 1u);
-                                umma_ts_i8(tmem + 2 * ACC_STRIDE, a0 + 16, smem_desc_plain(bw, lbo), idesc, acc);
-                                umma_ts_i8(tmem + 2 * ACC_STRIDE, a0 + 8, smem_desc_plain(bw + dstride, lbo), idesc, 1u);
-                                umma_ts_i8(tmem + 2 * ACC_STRIDE, a0, smem_desc_plain(bw + 2 * dstride, lbo), idesc, 1u);
+        // The whole warp runs the issue loop and polls the barriers together; one elected lane
+        // issues.  The tensor pipe queues only about two MMAs, so the loop is kept to a few
+        // instructions per MMA: the B descriptors move with the start address alone (bits 0-13,
+        // 16-byte units, no carry out for shared-memory addresses), the first anchor group of a
+        // sweep is peeled so that the accumulate flag is an immediate.
+        // S32 accumulate, signed int8 A and B, both K-major, M = 128, N = nmma
+        const uint32_t idesc = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(nmma >> 3) << 17) |
+                               ((uint32_t)(LS_ROWS >> 4) << 24);
+        const uint32_t lbo = (uint32_t)jd->span2 * 16;          // the second 16-pixel group of a digit
+        const uint64_t ddig = (uint64_t)((2 * lbo) >> 4);        // the next digit plane
+        const uint64_t desc0 = smem_desc_plain(smem_u32(smem + ST_D2), lbo) - (uint64_t)c0;  // row c0 at offset 0
+        const uint32_t accA = tmem, accB = tmem + ACC_STRIDE, accC = tmem + 2 * ACC_STRIDE;
+        const int ngr = g1 - g0;
+        int ns = 0, na = 0, ni = 0;
+        for (long b = u.b0; b < u.b1 && ok; ++b)
+            for (int sw = 0; sw < sweeps && ok; ++sw, ++ni) {
+                // the epilogue of the previous item has read the accumulators out
+                if (!mbar_wait_conv(acc_empty, (ni & 1) ^ 1, abort_flag, err, 32)) { ok = false; break; }
+                for (int sl = 0; sl < nslices(b) && ok; ++sl, ++ns) {
+                    const int s = ns % NSTAGE;
+                    if (!mbar_wait_conv(&st_full[s], (ns / NSTAGE) & 1, abort_flag, err, 33)) { ok = false; break; }
+                    const uint64_t sdesc = desc0 + (uint64_t)((s * ST_BYTES) >> 4);
+                    for (int g = 0; g < ngr; ++g, ++na) {
+                        const int ab = na % NABUF;
+                        if (!mbar_wait_conv(&ab_full[ab], (na / NABUF) & 1, abort_flag, err, 34)) { ok = false; break; }
+                        fence_after();
+                        const uint64_t q0 = sdesc + (uint64_t)sgroups[g], q1 = q0 + ddig, q2 = q1 + ddig;
+                        const uint32_t a0 = tmem + A_COL0 + ab * ABUF_COLS;
+                        if (sw == 0) {
+                            // class k = Σ_{i+j=k} Q_i·P_j into accumulator k
+                            if (sl == 0 && g == 0) {
+                                umma_i8_set(accA, a0, q0, idesc);
+                                umma_i8_set(accB, a0 + 8, q0, idesc);
+                                umma_i8_set(accC, a0 + 16, q0, idesc);
                             } else {
-                                // class 3: P3·Q0 + P2·Q1 + P1·Q2; the A buffer holds P1, P2, P3
-                                umma_ts_i8(tmem, a0 + 16, smem_desc_plain(bw, lbo), idesc, acc);
-                                umma_ts_i8(tmem, a0 + 8, smem_desc_plain(bw + dstride, lbo), idesc, 1u);
-                                umma_ts_i8(tmem, a0, smem_desc_plain(bw + 2 * dstride, lbo), idesc, 1u);
+                                umma_i8_add(accA, a0, q0, idesc);
+                                umma_i8_add(accB, a0 + 8, q0, idesc);
+                                umma_i8_add(accC, a0 + 16, q0, idesc);
                             }
-                            fresh = false;
-                            umma_commit(&ab_empty[ab]);
+                            umma_i8_add(accB, a0, q1, idesc);
+                            umma_i8_add(accC, a0 + 8, q1, idesc);
+                            umma_i8_add(accC, a0, q2, idesc);
+                        } else {
+                            // class 3: P3·Q0 + P2·Q1 + P1·Q2; the A buffer holds P1, P2, P3
+                            if (sl == 0 && g == 0) umma_i8_set(accA, a0 + 16, q0, idesc);
+                            else umma_i8_add(accA, a0 + 16, q0, idesc);
+                            umma_i8_add(accA, a0 + 8, q1, idesc);
+                            umma_i8_add(accA, a0, q2, idesc);
                         }
-                        if (ok) umma_commit(&st_empty[s]);
+                        umma_commit_elect(&ab_empty[ab]);
                     }
-                    if (ok) umma_commit(acc_full);
+                    if (ok) umma_commit_elect(&st_empty[s]);
                 }
-            if (!ok) {
-                umma_commit(drain);
-                for (long long i = 0; i < WAIT_LIMIT && !mbar_try_wait(drain, 0); ++i) __nanosleep(100);
+                if (ok) umma_commit_elect(acc_full);
             }
+        if (!ok) {
+            umma_commit_elect(drain);
+            if (lane == 0)
+                for (long long i = 0; i < WAIT_LIMIT && !mbar_try_wait(drain, 0); ++i) __nanosleep(100);
+            __syncwarp();
         }
     } else {
         // ---- warps 0-15: form the A digits, then each block's epilogue ----
@@ -301,14 +341,14 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         const int a = ks > 1 ? r / nclen : 0;             // anchor slot of the row
         const int d3 = ks > 1 ? r % nclen : r;            // lag Δ3 within the tile
         const bool row_ok = r < mrows;
-        const int row0_3 = c0 - jd->nc10 + (ks > 1 ? 0 : LS_ROWS * u.t3);  // channel of staged D3 row 0
         const uint32_t lane_field = (uint32_t)(32 * q) << 16;
         const int ngr = g1 - g0, nab1 = c1 - c0;
         int ns = 0, na = 0, ni = 0;
         // One iteration fills the A buffers of two anchor groups (one barrier round trip, one
-        // tcgen05.wait::st); lanes whose row has no data (past the tile, past the anchor block,
-        // or a D3 channel outside [0, nc)) store zero digits, and a warp with no such lane skips
-        // the arithmetic.
+        // tcgen05.wait::st).  A lane whose row has no data (past the tile or past the anchor
+        // block) reads a zeroed row, so its digits come out zero with no per-digit select; D3
+        // channels outside [0, nc) arrive as zero rows from the TMA bounds fill.  A warp with no
+        // such lane skips the arithmetic.
         auto form_slice = [&](auto ndc, const unsigned char *st) {
             constexpr int ND = decltype(ndc)::value;
             for (int gi = 0; gi < ngr && ok; gi += 2) {
@@ -326,12 +366,9 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                     if (h >= nb2) break;
                     const int p1 = sgroups[gi + h] + a;
                     const int rho = p1 - c0 + d3;  // staged D3 row of this lane
-                    const int p3 = row0_3 + rho;
-                    const bool valid = row_ok && p1 < c1 && p3 >= 0 && p3 < nc;
-#pragma unroll
-                    for (int dd = 0; dd < 3; ++dd) w[h][dd][0] = w[h][dd][1] = 0u;
+                    const bool valid = row_ok && p1 < c1;
                     if (__any_sync(0xffffffffu, valid)) {
-                        const unsigned char *row3 = st + ST_D3 + min(rho, LS_SPAN - 1) * 128;
+                        const unsigned char *row3 = valid ? st + ST_D3 + rho * 128 : zero_row;
                         const float4 x0 = *reinterpret_cast<const float4 *>(row3 + (((2 * ps) ^ (rho & 7)) << 4));
                         const float4 x1 = *reinterpret_cast<const float4 *>(row3 + (((2 * ps + 1) ^ (rho & 7)) << 4));
                         // the D1 row, already scaled by 127·2^−(E1+E3) for this block
@@ -346,13 +383,12 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                         constexpr int D0 = ND - 3;  // sweep 2 stores product digits 1-3
 #pragma unroll
                         for (int dd = 0; dd < 3; ++dd) {
-                            w[h][dd][0] = valid ? pack_low_bytes(ya[dd + D0].x, ya[dd + D0].y, yb[dd + D0].x,
-                                                                 yb[dd + D0].y)
-                                                : 0u;
-                            w[h][dd][1] = valid ? pack_low_bytes(yc[dd + D0].x, yc[dd + D0].y, yd[dd + D0].x,
-                                                                 yd[dd + D0].y)
-                                                : 0u;
+                            w[h][dd][0] = pack_low_bytes(ya[dd + D0].x, ya[dd + D0].y, yb[dd + D0].x, yb[dd + D0].y);
+                            w[h][dd][1] = pack_low_bytes(yc[dd + D0].x, yc[dd + D0].y, yd[dd + D0].x, yd[dd + D0].y);
                         }
+                    } else {
+#pragma unroll
+                        for (int dd = 0; dd < 3; ++dd) w[h][dd][0] = w[h][dd][1] = 0u;
                     }
                     // pixels 8ps .. 8ps+7 of the slice = columns 2ps, 2ps+1 of each digit's 8
                     const uint32_t col = tmem + lane_field + A_COL0 + ((na + h) % NABUF) * ABUF_COLS + 2 * ps;
@@ -429,7 +465,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     }
 }
 
-constexpr size_t SMEM_BYTES = 1024 + (size_t)NSTAGE * ST_BYTES + 256 + sizeof(int) * LS_SPAN;
+constexpr size_t SMEM_BYTES = 1024 + (size_t)NSTAGE * ST_BYTES + 256 + sizeof(int) * LS_SPAN + 128;
 
 typedef CUresult (*EncodeTiled)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
                                 const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,

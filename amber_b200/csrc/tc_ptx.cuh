@@ -70,6 +70,24 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volati
     return false;
 }
 
+// Bounded wait for a converged warp: every lane polls the same barrier and the
+// warp leaves the loop together, so it stays converged for the elect.sync-issued
+// tcgen05 ops that follow and no broadcast of the answer is needed.
+__device__ __forceinline__ bool mbar_wait_conv(uint64_t *bar, uint32_t parity, volatile int *abort_flag, int *err,
+                                               int code)
+{
+    if (__all_sync(0xffffffffu, mbar_try_wait(bar, parity))) return true;
+    const long long t0 = clock64();
+    while (true) {
+        if (__all_sync(0xffffffffu, mbar_try_wait_sleep(bar, parity))) return true;
+        if (__any_sync(0xffffffffu, *abort_flag != 0)) return false;
+        if (__any_sync(0xffffffffu, clock64() - t0 > WAIT_CYCLES)) break;
+    }
+    *abort_flag = 1;
+    atomicExch(err, code);
+    return false;
+}
+
 // Warp-uniform bounded wait: lane 0 polls, every lane gets the same answer, so
 // the warp stays converged for the .sync.aligned tcgen05 ops that follow.
 __device__ __forceinline__ bool mbar_wait_warp(uint64_t *bar, uint32_t parity, volatile int *abort_flag, int *err,
