@@ -289,7 +289,7 @@ void Engine::loop()
         }
         const double t0 = now_ms();
         // this round's share of the statistics, published under the lock at its end
-        double setup_ms = 0, maps_ms = 0, contract_ms = 0, finish_ms = 0;
+        double setup_ms = 0, maps_ms = 0, contract_ms = 0, finish_ms = 0, kernel_ms = 0;
         long launches = 0, all_launches = 0;
         owner->phase_used = 0;  // per-phase timing events are reused round after round
         // one map-set batch of every active request
@@ -309,9 +309,20 @@ void Engine::loop()
             }
             if (!rc) {
                 ta = now_ms();
-                const long launched = r->sub->launches;
+                const long launched = r->sub->launches, contracted = r->sub->contractions;
+                r->sub->phase_used = 0;
                 rc = run_next_batch(r->sub, r->run, &jobs);
                 all_launches += r->sub->launches - launched;
+                launches += r->sub->contractions - contracted;
+                // contractions that ran inside the request's own context (the FP64 paths): their
+                // kernel time, from the phase events around each launch
+                for (size_t i = 0; i < r->sub->phase_used; ++i)
+                    if (r->sub->phase_ev[i].phase == 1 && cudaEventSynchronize(r->sub->phase_ev[i].b) == cudaSuccess) {
+                        float ms = 0;
+                        if (cudaEventElapsedTime(&ms, r->sub->phase_ev[i].a, r->sub->phase_ev[i].b) == cudaSuccess)
+                            kernel_ms += ms;
+                    }
+                cudaGetLastError();
                 rc = rc < 0 ? rc : AMBER_OK;
                 maps_ms += now_ms() - ta;
             }
@@ -323,11 +334,10 @@ void Engine::loop()
         }
         int rc = AMBER_OK;
         double tc = now_ms();
-        double kernel_ms = 0;
         if (!jobs.empty()) {
             const long before = owner->contractions, launched = owner->launches;
             rc = contract_i8_jobs(owner, jobs);  // synchronises the stream
-            launches = owner->contractions - before;
+            launches += owner->contractions - before;
             all_launches += owner->launches - launched;
             for (size_t i = 0; i < owner->phase_used; ++i)
                 if (owner->phase_ev[i].phase == 1) {

@@ -1,36 +1,42 @@
 """Benchmark of the AMBER estimator hot path on B200.
 
-Workload (one "step"): the single-realisation case — a 256² uv grid, 128
-channels (channels 0-1 and 30-31 of every 32-channel block flagged), 16
-log-spaced annular bins from 2 to 120 cells, all lag pairs |Δν| < 64
-(nc10 = 63), v2 output — pushed through the whole estimator: calCR, then for
-all 218 closed triangles the ring maps and the triple-product lag
-accumulation of both the visibility maps (bldnu) and the sampling-mask maps
-(numdnu).  Inputs are seeded synthetic data of that shape (there is no
+Workload (the headline): the batched ensemble — 64 realisations of uneven size,
+grid side drawn from {96, 128, 192, 256, 320}, 24-160 channels, random 10 %
+channel flags, 12 log-spaced annular bins from 2 to 0.47·side cells, all lag
+pairs |Δν| ≤ nc/2 − 1, v2 output (visibility sums bldnu and sampling-mask sums
+numtri), seeds 100-163.  Every realisation goes through the whole estimator:
+calCR, then for all closed triangles the ring maps and the triple-product lag
+accumulation.  Inputs are seeded synthetic data of that shape (there is no
 public dataset for this path).
+
+One step = one batch of 8 realisations (realisations j, j+8, …, j+56 for batch
+j, so every batch mixes grid sizes) through the request engine; the default
+K = 8 steps time the whole ensemble exactly once after W = 3 warm-up batches.
 
 Metric: lag-triple products per second, one product being one term
 D_r1(x,p1)·D_r2(x,p2)·D_r3(x,p3) of the reference's loop (4_fbe/amber.c:261-263);
 per triangle total_vcp·Ng1², counted for the D and the I (mask) sums.
 
-* value — device time of the run with the grid already resident in HBM;
-* e2e   — the same through the C ABI from pinned host buffers: grid upload and
-  normalisation, rings, channels, calCR, the run, and the copy of every lag
-  array back to the host, all inside the timed region;
-* fp64_plain — the plain FP64 GPU path on the same GPU over a bounded sample;
-* roofline — the contraction kernel, algorithmic flops (2 per product) per
-  launch over its CUDA-event time, against the measured bf16 dense peak;
+* value — device time (CUDA events) of the steps with every cube already in HBM
+  (amber_cuda_enqueue with inputs_on_device);
+* e2e   — the same steps through the public API from host memory: each request's
+  cube copied in, every lag array (bldnu, numdnu, numtri) copied back;
+* fp64_plain — the plain FP64 GPU path over the whole ensemble, its contraction
+  kernel's rate against the measured FP64 GEMM peak, and the mixed path's error
+  against it on three realisations;
+* roofline — the int8 contraction kernel, algorithmic flops (2 per product) over
+  its CUDA-event time, against the measured bf16 dense peak;
 * cpu_baseline — the reference's own OpenMP loop (oracle/_ref/ref_amber_fast,
-  its sources built unchanged) on the host cores over a bounded sample;
-* ensemble — 64 realisations of uneven size through the request engine
-  (amber_cuda_enqueue), end to end, with mixed vs plain FP64 on a subset;
-* serving — a prefix of the Poisson request stream enqueued at its arrival
-  times: p50/p99 latency and throughput, FP64 one-at-a-time beside it.
+  its sources built unchanged) on the host cores, one triangle of the ensemble;
+* single_realisation — the 256², 128-channel, 16-bin realisation on the
+  device-resident path.
 
 `--impl reference` times that same reference build as the reference arm.
-Multi-GPU: one process per GPU (torchrun), each rank runs its own realisation
-(seed 1 + rank): weak scaling, no collective on the data path; timing is the
-max over ranks.
+`--serving N`, `--config4`, `--config1`, `--stages`, `--maps`, `--gridding` run
+the other measurements instead of the headline.
+Multi-GPU: one process per GPU (torchrun); each rank runs its own ensemble
+(seeds 100 + 64·rank onwards): weak scaling, no collective on the data path;
+timing is the max over ranks.
 """
 from __future__ import annotations
 
@@ -51,15 +57,18 @@ sys.path.insert(0, ROOT)
 
 METRIC = "lag-triple products/s vs plain FP64 on same GPU @<=1e-6 rel err; p50/p99 latency"
 UNIT = "lag-triple products/s"
-WORKLOAD = dict(workload="single realisation: 256^2 grid, 128 channels (4 of every 32 flagged), "
-                         "16 log bins 2-120 cells, nc10=63, v2 (D and mask sums), all 218 closed triangles",
-                grid=256, channels=128, bins=16, nc10=63, du=0.5, version=2)
+WORKLOAD = dict(workload="batched ensemble: 64 realisations, sides {96,128,192,256,320}, 24-160 channels, "
+                         "10 % random channel flags, 12 log bins 2..0.47*side cells, nc10=nc/2-1, v2 (D and mask "
+                         "sums), all closed triangles, seeds 100-163; step = 8 realisations",
+                realisations=64, batch=8, bins=12, version=2)
+SINGLE = "single realisation: 256^2 grid, 128 channels (4 of every 32 flagged), 16 log bins 2-120 cells, nc10=63, v2"
 
 
-# DRAM bytes per lag-triple product of contract_i8_kernel, from one ncu capture of a full launch
-# (triangle rp=140 of the single-realisation workload: 227.51 MB for 810152 * 125316 products).
-# Every map row is read once per launch, so traffic grows with products.
-DRAM_BYTES_PER_PRODUCT = 227.51e6 / (810152 * 125316)
+# DRAM bytes per lag-triple product of the int8 lag-space kernel (ls_i8_kernel), from one ncu capture
+# of a full launch (profiles/ls_i8_kernel_config2_one_triangle.txt): every staged map slice is read
+# once per unit, so traffic grows with the products of a launch.
+DRAM_BYTES_PER_PRODUCT = (493.735e6 + 26.335e6) / 4.436392352e11
+CPU_SAMPLE_REALISATION = 3  # side 256, 116 channels: its last (largest-ring) triangle is ~15 s of reference CPU
 
 
 def peaks():
@@ -126,8 +135,12 @@ def cpu_reference_sample(real, nthreads=None, rp_pick=None, version=1, fast=True
     try:
         nthreads = nthreads or os.cpu_count() or 1
         if rp_pick is None:
-            # the last triangle: largest ring r1 = 15, Ng1 = 740 — the kind of triangle that dominates the step
-            rp_pick = len(oracle.triangles(real.ulow, real.uhigh)) - 1
+            # the last closed triangle of the build being timed (its own calCR: the float build's
+            # list can be one shorter than the FP64 one), found by a run over no triangles: the
+            # largest ring r1, the kind of triangle that dominates a realisation
+            st0, _ = oracle.run_ref_amber(real, wd, version=version, fp64=False, fast=fast, rp_begin=0, rp_end=0,
+                                          nthreads=nthreads)
+            rp_pick = int(st0["rcount"]) - 1
         st, _ = oracle.run_ref_amber(real, wd, version=version, fp64=False, fast=fast, rp_begin=rp_pick,
                                      rp_end=rp_pick + 1, nthreads=nthreads)
         return st, rp_pick
@@ -144,7 +157,7 @@ def run_reference_arm(args):
     if not oracle.ref_available():
         print(json.dumps({"impl": "reference", "unavailable": "reference build oracle/_ref missing (make -C oracle ref)"}))
         return 0
-    real = synth.config2()
+    real = synth.from_spec(synth.config3_specs()[CPU_SAMPLE_REALISATION])
     rates, times = [], []
     st = None
     for i in range(args.warmup + args.steps):
@@ -154,8 +167,8 @@ def run_reference_arm(args):
             rates.append(rate)
             times.append(st["accum_s"])
     value = float(np.median(rates))
-    sample = (f"triangle rp={rp} of the workload (Ng1=740, total_vcp={st['total_vcp']}), v1 accumulation loop "
-              f"timed like amber.c:230,285; maps excluded")
+    sample = (f"ensemble realisation {CPU_SAMPLE_REALISATION} (side {real.nn}, {real.nc} channels), its last triangle "
+              f"rp={rp} (total_vcp={st['total_vcp']}), v1 accumulation loop timed like amber.c:230,285; maps excluded")
     out = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * float(np.median(times)),
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
@@ -167,90 +180,126 @@ def run_reference_arm(args):
     return 0
 
 
-def _engine_run(amber_b200, reals, precision, dev):
-    """All realisations through one context's request engine; returns (wall s, products, results, stats)."""
-    with amber_b200.Estimator(device=dev, precision=precision) as est:
+def ensemble_batches(n=64, b=8):
+    """Batch j holds realisations j, j+b, j+2b, …: every batch mixes grid sizes."""
+    return [list(range(j, n, b)) for j in range(b)]
+
+
+def run_batch(eng, reals, idx, cubes=None):
+    """Enqueue the realisations ``idx`` (device-resident when ``cubes`` is given), wait for all of
+    them and read their results back; returns the results in ``idx`` order."""
+    tickets = [eng.enqueue(reals[i], want_v2=True, device_cube=None if cubes is None else cubes[i]) for i in idx]
+    return [eng.result(t, reals[i], want_v2=True) for t, i in zip(tickets, idx)]
+
+
+def device_cubes(torch, reals, dev):
+    """Each realisation's summed grid and counts as device tensors (the packed layout the engine reads)."""
+    keep, ptrs = [], []
+    for r in reals:
+        ri = torch.from_numpy(np.ascontiguousarray(r.gv).view(np.float64)).to(dev)
+        nt = torch.from_numpy(np.ascontiguousarray(r.counts, dtype=np.float64)).to(dev)
+        keep.append((ri, nt))
+        ptrs.append((ri.data_ptr(), nt.data_ptr()))
+    return keep, ptrs
+
+
+def fp64_peak(torch, dev, n=8192, reps=5):
+    """Measured FP64 dense rate of the GPU: a float64 n³ matmul, best of ``reps`` (TFLOP/s)."""
+    a = torch.randn(n, n, dtype=torch.float64, device=dev)
+    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    torch.matmul(a, b)
+    best = 0.0
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize(dev)
+        best = max(best, 2.0 * n ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+    del a, b
+    return best
+
+
+def fp64_section(amber_b200, torch, reals, cubes, dev, mixed_sub):
+    """The plain FP64 path over the whole ensemble (same engine, device-resident cubes), its
+    contraction kernel's rate against the measured FP64 GEMM peak, and the mixed path's error
+    against it on the realisations ``mixed_sub`` (a dict index -> mixed result)."""
+    peak = fp64_peak(torch, dev)
+    with amber_b200.Estimator(device=dev, precision="fp64") as est:
         eng = amber_b200.Engine(est)
-        p0 = eng.stats()["products"]
+        run_batch(eng, reals, [min(range(len(reals)), key=lambda i: reals[i].nn * reals[i].nc)], cubes)  # warm-up
+        s0 = eng.stats()
         t0 = time.perf_counter()
-        tickets = [eng.enqueue(r, want_v2=True) for r in reals]
-        res = [eng.result(t, r, want_v2=True) for t, r in zip(tickets, reals)]
+        res = run_batch(eng, reals, list(range(len(reals))), cubes)
         wall = time.perf_counter() - t0
-        st = eng.stats()
-    return wall, st["products"] - p0, res, st
-
-
-def ensemble_section(amber_b200, synth, dev):
-    """Batched ensemble: the 64 realisations of uneven size (sides 96-320, 24-160 channels, 10 %
-    flags, 12 bins) through the request engine, end to end (inputs from host memory, every lag
-    array back); plus mixed vs plain FP64 on a fixed subset of the same ensemble."""
-    specs = synth.config3_specs()
-    t_gen = time.perf_counter()
-    reals = [synth.from_spec(s) for s in specs]
-    t_gen = time.perf_counter() - t_gen
-    _engine_run(amber_b200, reals[48:49], "mixed", dev)  # warm-up (allocations, twiddles)
-    wall, prod, _, st = _engine_run(amber_b200, reals, "mixed", dev)
-    sub = [0, 16, 48]
-    sreals = [reals[i] for i in sub]
-    w_m, p_m, r_m, _ = _engine_run(amber_b200, sreals, "mixed", dev)
-    w_f, p_f, r_f, _ = _engine_run(amber_b200, sreals, "fp64", dev)
-    _, _, r_a, _ = _engine_run(amber_b200, sreals, "fp64_abs", dev)
+        s1 = eng.stats()
+    prod = s1["products"] - s0["products"]
+    kms = s1["contract_kernel_ms"] - s0["contract_kernel_ms"]
+    achieved = 2.0 * prod / (kms * 1e-3) / 1e12 if kms > 0 else None
     err = 0.0
-    for m, f, a in zip(r_m, r_f, r_a):
-        err = max(err, float((np.abs(m[1] - f[1]) / (a[1] + 1e-300)).max()),
-                  float((np.abs(m[3] - f[3]) / (a[3] + 1e-300)).max()))
-        assert np.array_equal(m[2], f[2])  # counts exact
-    return {"workload": "ensemble: 64 realisations, sides {96,128,192,256,320}, 24-160 channels, 10 % flags, "
-                        "12 log bins 2..0.47*side, nc10=nc/2-1, v2, all closed triangles, seeds 100-163",
-            "value": prod / wall, "unit": UNIT, "products": prod, "wall_s": wall,
-            "timing": "end to end through amber_cuda_enqueue/wait/result from host memory (wall clock)",
-            "engine": {k: st[k] for k in ("rounds", "contraction_launches", "max_active", "peak_bytes", "busy_ms",
-                                          "setup_ms", "maps_ms", "contract_ms", "finish_ms")},
-            "fp64_plain": {"sample": "realisations 0, 16, 48 of the ensemble (sides 256/192/96), same engine",
-                           "value": p_f / w_f, "mixed_same_sample": p_m / w_m, "speedup": (p_m / w_m) / (p_f / w_f),
-                           "max_rel_err_vs_fp64": err, "err_scale": "sum of |products| per lag cell"},
-            "generation_s": t_gen}
+    with amber_b200.Estimator(device=dev, precision="fp64_abs") as est:
+        eng = amber_b200.Engine(est)
+        for i, m in mixed_sub.items():
+            a = run_batch(eng, reals, [i], cubes)[0]
+            f = res[i]
+            err = max(err, float((np.abs(m[1] - f[1]) / (a[1] + 1e-300)).max()),
+                      float((np.abs(m[3] - f[3]) / (a[3] + 1e-300)).max()))
+            assert np.array_equal(m[2], f[2])  # counts exact
+    return {"value": prod / wall, "unit": UNIT, "products": prod, "wall_s": wall,
+            "sample": "the whole ensemble (64 realisations), same engine, device-resident cubes",
+            "kernel": {"name": "ls_fp64_kernel", "achieved_tflops": achieved, "peak_tflops": peak,
+                       "frac": None if achieved is None else achieved / peak,
+                       "peak_kind": "measured here: torch float64 8192^3 matmul, best of 5",
+                       "flops": "2 per lag-triple product (useful products only; lag-window padding excluded)"},
+            "max_rel_err_vs_fp64": err, "err_scale": "sum of |products| per lag cell",
+            "err_sample": sorted(mixed_sub)}
 
 
-def serving_section(amber_b200, synth, dev, n=8):
-    """Serving stream: the first n requests of the Poisson stream (50 req/s; sides {64..384},
-    16-256 channels, 6-20 bins) enqueued at their arrival times; latency = arrival to result
-    ready.  The stream as specified is far beyond one GPU's capacity (~1.5e17 products arriving
-    in 39 s), so only a prefix runs; the plain FP64 one-at-a-time path is timed on two small
-    requests of the prefix."""
+def serving_section(amber_b200, synth, dev, n=200, rate=0.2):
+    """Serving stream: ``n`` requests of the config-5 size distribution (sides {64,128,256,384},
+    16-256 channels, 6-20 bins, own seed and flags) arriving as a Poisson process at ``rate``
+    req/s (the stream's 50 req/s inter-arrival times rescaled), enqueued at their arrival times;
+    latency = arrival to result ready.  The plain FP64 path one request at a time runs on the ten
+    smallest requests of the same sample."""
     reqs = synth.config5_requests()[:n]
+    t_gen = time.perf_counter()
     reals = [synth.from_spec(q) for q in reqs]
-    _engine_run(amber_b200, [synth.from_spec(dict(reqs[4], nn=64))], "mixed", dev)  # warm-up
+    t_gen = time.perf_counter() - t_gen
+    scale = 50.0 / rate
     with amber_b200.Estimator(device=dev, precision="mixed") as est:
         eng = amber_b200.Engine(est)
-        p0 = eng.stats()["products"]
+        run_batch(eng, [synth.from_spec(dict(reqs[0], nn=64, nc=32))], [0])  # warm-up
+        s0 = eng.stats()
         t0 = time.perf_counter()
         tickets = []
         for q, r in zip(reqs, reals):
-            delay = (q["arrival"] - reqs[0]["arrival"]) - (time.perf_counter() - t0)
+            delay = scale * (q["arrival"] - reqs[0]["arrival"]) - (time.perf_counter() - t0)
             if delay > 0:
                 time.sleep(delay)
             tickets.append(eng.enqueue(r, want_v2=True))
         lat = [eng.result(t, r, want_v2=True)[4] for t, r in zip(tickets, reals)]
         wall = time.perf_counter() - t0
-        st = eng.stats()
-        prod = st["products"] - p0
-    small = sorted(range(n), key=lambda i: reqs[i]["nn"] ** 2 * reqs[i]["nc"] * reqs[i]["nbins"])[:2]
+        s1 = eng.stats()
+    prod = s1["products"] - s0["products"]
+    small = sorted(range(n), key=lambda i: reqs[i]["nn"] ** 2 * reqs[i]["nc"] ** 3 * reqs[i]["nbins"])[:10]
     f_prod, f_wall, f_lat = 0.0, 0.0, []
-    for i in small:
-        with amber_b200.Estimator(device=dev, precision="fp64") as e64:
+    with amber_b200.Estimator(device=dev, precision="fp64") as e64:
+        amber_b200.estimate(reals[small[0]], precision="fp64", version=2, est=e64)  # warm-up
+        for i in small:
             t = time.perf_counter()
             amber_b200.estimate(reals[i], precision="fp64", version=2, est=e64)
             f_lat.append(1e3 * (time.perf_counter() - t))
             f_prod += e64.last_run_stats()[0]
             f_wall += time.perf_counter() - t
-    return {"workload": f"serving: first {n} requests of the Poisson stream (50 req/s), sides/channels/bins as drawn",
-            "requests": n, "value": prod / wall, "unit": UNIT, "products": prod, "wall_s": wall,
+    return {"workload": f"serving: {n} requests of the config-5 size distribution, Poisson arrivals at {rate} req/s",
+            "requests": n, "rate_req_s": rate, "value": prod / wall, "unit": UNIT, "products": prod, "wall_s": wall,
             "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-            "latency_ms": [round(x, 1) for x in lat],
-            "engine": {k: st[k] for k in ("rounds", "contraction_launches", "max_active", "peak_bytes")},
-            "fp64_one_at_a_time": {"requests": small, "value": f_prod / f_wall, "latency_ms": f_lat,
-                                   "sizes": [(reqs[i]["nn"], reqs[i]["nc"], reqs[i]["nbins"]) for i in small]}}
+            "mixed_latency_ms_of_fp64_sample": [round(lat[i], 1) for i in small],
+            "engine": {k: s1[k] - s0[k] if k in ("rounds", "contraction_launches") else s1[k]
+                       for k in ("rounds", "contraction_launches", "max_active", "peak_bytes")},
+            "fp64_one_at_a_time": {"requests": small, "value": f_prod / f_wall, "latency_ms": [round(x, 1) for x in f_lat],
+                                   "p50_ms": float(np.percentile(f_lat, 50))},
+            "generation_s": t_gen}
 
 
 def config4_section(amber_b200, synth, dev, args):
@@ -428,30 +477,57 @@ def maps_section(amber_b200, synth, dev):
     return res
 
 
+def single_section(amber_b200, synth, dev, stream, reps=2):
+    """The single-realisation case on the device-resident path: all 218 closed triangles of the
+    256² realisation, one warm-up run and ``reps`` timed runs (CUDA events)."""
+    import torch
+    real = synth.config2(seed=1)
+    with amber_b200.Estimator(device=dev, precision="mixed", stream=stream.cuda_stream) as est:
+        est.load_grid(real.gv, real.counts, real.du, real.flag_key)
+        est.set_rings(real.ulow, real.uhigh)
+        est.set_channels(real.nc10, real.uf_chans)
+        tri = est.calcr()[:, :3].astype(np.int32)
+        est.run(tri, want_v2=True)
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        prod, cms = 0.0, 0.0
+        for _ in range(reps):
+            est.run(tri, want_v2=True)
+            prod += est.last_run_stats()[0]
+            cms += est.last_run_breakdown()[1]
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        ms = e0.elapsed_time(e1)
+    return {"workload": SINGLE, "value": prod / (ms * 1e-3), "unit": UNIT, "ms_per_run": ms / reps,
+            "contract_ms_per_run": cms / reps, "products_per_run": prod / reps}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=8, help="timed batches of 8 realisations (8 = the whole ensemble)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="amber_b200", choices=["amber_b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
-    ap.add_argument("--tri-subset", default="", help="comma-separated triangle indices (profiling runs only)")
-    ap.add_argument("--tile-n", type=int, default=0, choices=[0, 32, 64, 128],
-                    help="fix the contraction's p3 tile width instead of the autotuner's choice (profiling runs: "
-                         "under a profiler the tuner's trial timings are not representative)")
-    ap.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble measurement")
-    ap.add_argument("--no-serving", action="store_true", help="skip the serving-stream measurement")
+    ap.add_argument("--no-single", action="store_true", help="skip the single-realisation section")
+    ap.add_argument("--serving", type=int, default=0, metavar="N",
+                    help="run N requests of the serving stream instead of the headline")
+    ap.add_argument("--rate", type=float, default=0.2, help="Poisson arrival rate of --serving (req/s)")
     ap.add_argument("--config1", action="store_true",
                     help="measure the reference's whole CPU-runnable case (config 1) beside the reference's own run")
     ap.add_argument("--stages", action="store_true",
                     help="time the stages beside the contraction (cylindrical bispectra, gridding with collapse)")
     ap.add_argument("--maps", action="store_true",
-                    help="measure the MAPS two-point function (amber_cuda_cl_dnu) instead of the default step")
+                    help="measure the MAPS two-point function (amber_cuda_cl_dnu) instead of the headline")
     ap.add_argument("--gridding", action="store_true",
                     help="time the gridding stage alone (100k records x 128 channels onto 256^2)")
     ap.add_argument("--config4", action="store_true",
-                    help="measure a fixed sample of the large cube (512^2, 384 channels) instead of the default step")
+                    help="measure a fixed sample of the large cube (512^2, 384 channels) instead of the headline")
+    ap.add_argument("--profile-triangle", type=int, default=-1, metavar="RP",
+                    help="profiling runs: triangle RP of the single-realisation case, twice, v1, on --precision")
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -464,226 +540,182 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     build.build()
 
-    if args.config4:
-        if rank == 0:
-            c4 = config4_section(amber_b200, synth, local, args)
-            print(json.dumps(dict(metric=METRIC, impl="amber_b200", n_gpus=1, higher_is_better=True,
-                                  dtype="int8 tensor-core digits, int32 accumulate, fp64 reduce", data="synthetic",
-                                  config={"workload": c4["workload"]}, **{k: v for k, v in c4.items() if k != "workload"})))
+    if args.profile_triangle >= 0:
+        real = synth.config2(seed=1)
+        with amber_b200.Estimator(device=local, precision=args.precision) as est:
+            est.load_grid(real.gv, real.counts, real.du, real.flag_key)
+            est.set_rings(real.ulow, real.uhigh)
+            est.set_channels(real.nc10, real.uf_chans)
+            tri = est.calcr()[[args.profile_triangle], :3].astype(np.int32)
+            for _ in range(2):  # a profiler captures the second launch (-s 1)
+                est.run(tri, want_v2=False)
+            p, ms = est.last_run_stats()
+        print(json.dumps({"profile_triangle": args.profile_triangle, "precision": args.precision,
+                          "products": p, "ms": ms}))
         return 0
 
-    if args.config1:
-        if rank == 0:
-            c1 = config1_section(amber_b200, synth, local)
-            print(json.dumps(dict(metric=METRIC, impl="amber_b200", n_gpus=1, higher_is_better=True, data="synthetic",
-                                  config={"workload": c1["workload"]}, **{k: v for k, v in c1.items() if k != "workload"})))
-        return 0
+    modes = (("config4", lambda: config4_section(amber_b200, synth, local, args)),
+             ("config1", lambda: config1_section(amber_b200, synth, local)),
+             ("stages", lambda: stages_section(amber_b200, synth, local)),
+             ("gridding", lambda: gridding_section(amber_b200, synth, local)),
+             ("maps", lambda: maps_section(amber_b200, synth, local)),
+             ("serving", lambda: serving_section(amber_b200, synth, local, n=args.serving, rate=args.rate)))
+    for name, fn in modes:
+        if getattr(args, name):
+            if rank == 0:
+                r = fn()
+                print(json.dumps(dict(metric=METRIC, impl="amber_b200", n_gpus=1, data="synthetic",
+                                      config={"workload": r["workload"]},
+                                      **{k: v for k, v in r.items() if k != "workload"})))
+            return 0
 
-    if args.stages:
-        if rank == 0:
-            st = stages_section(amber_b200, synth, local)
-            print(json.dumps(dict(impl="amber_b200", n_gpus=1, data="synthetic", config={"workload": st["workload"]},
-                                  **{k: v for k, v in st.items() if k != "workload"})))
-        return 0
-
-    if args.gridding:
-        if rank == 0:
-            gr = gridding_section(amber_b200, synth, local)
-            print(json.dumps(dict(impl="amber_b200", n_gpus=1, dtype="f64 sums of f32 records", data="synthetic",
-                                  config={"workload": gr["workload"]}, **{k: v for k, v in gr.items() if k != "workload"})))
-        return 0
-
-    if args.maps:
-        if rank == 0:
-            m = maps_section(amber_b200, synth, local)
-            print(json.dumps(dict(impl="amber_b200", n_gpus=1, dtype="f64", data="synthetic",
-                                  config={"workload": m["workload"]}, **{k: v for k, v in m.items() if k != "workload"})))
-        return 0
-
-    real = synth.config2(seed=1 + rank)
-    stream = torch.cuda.current_stream(dev)
-    est = amber_b200.Estimator(device=local, precision="mixed", stream=stream.cuda_stream, tile_n=args.tile_n)
-    est.load_grid(real.gv, real.counts, real.du, real.flag_key)
-    est.set_rings(real.ulow, real.uhigh)
-    est.set_channels(real.nc10, real.uf_chans)
-    rdata = est.calcr()
-    tri = rdata[:, :3].astype(np.int32)
-    if args.tri_subset:
-        tri = tri[[int(t) for t in args.tri_subset.split(",")]]
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # 256 MB > 126 MB L2
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
 
     def barrier():
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize(dev)
 
-    def max_over_ranks(x):
+    def reduce(x, op):
         if world == 1:
             return x
         t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(t, op=op)
         return float(t.item())
 
-    def sum_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        return float(t.item())
+    # ---- this rank's ensemble, its cubes resident in HBM ----
+    t_gen = time.perf_counter()
+    specs = synth.config3_specs(seed0=100 + 64 * rank)
+    reals = [synth.from_spec(sp) for sp in specs]
+    t_gen = time.perf_counter() - t_gen
+    keep, cubes = device_cubes(torch, reals, dev)
+    batches = ensemble_batches(len(reals), 8)
+    order = [batches[(args.warmup + k) % len(batches)] for k in range(args.steps)]
+    stream = torch.cuda.current_stream(dev)
+    est = amber_b200.Estimator(device=local, precision="mixed")
+    eng = amber_b200.Engine(est)
 
     # ---- device-resident throughput (value) ----
-    for _ in range(args.warmup):
-        flush.zero_()
-        est.run(tri, want_v2=True)
+    for k in range(args.warmup):
+        run_batch(eng, reals, batches[k % len(batches)], cubes)
     clocks = Clocks(local)
     clocks.start()
     barrier()
+    s0 = eng.stats()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    products = 0.0
-    contract_ms = maps_ms = reduce_ms = 0.0
-    launches = contracts = 0
-    step_ms = []
-    for _ in range(args.steps):
-        flush.zero_()
-        est.run(tri, want_v2=True)
-        p, ms = est.last_run_stats()
-        a, b, c, n, m = est.last_run_breakdown()
-        products += p
-        step_ms.append(ms)
-        maps_ms += a
-        contract_ms += b
-        reduce_ms += c
-        launches += n + 1  # + the L2 flush kernel
-        contracts += m
+    mixed = {}
+    for idx in order:
+        for i, r in zip(idx, run_batch(eng, reals, idx, cubes)):
+            mixed[i] = r
     e1.record(stream)
     barrier()
     clk = clocks.stop()
-    total_ms = max_over_ranks(e0.elapsed_time(e1))
-    all_products = sum_over_ranks(products)
+    s1 = eng.stats()
+    total_ms = reduce(e0.elapsed_time(e1), dist.ReduceOp.MAX if world > 1 else None)
+    products = s1["products"] - s0["products"]
+    all_products = reduce(products, dist.ReduceOp.SUM if world > 1 else None)
     value = all_products / (total_ms * 1e-3)
+    kms = s1["contract_kernel_ms"] - s0["contract_kernel_ms"]
+    launches = s1["contraction_launches"] - s0["contraction_launches"]
+    gpu_launches = s1["kernel_launches"] - s0["kernel_launches"]
 
-    # ---- end to end through the C ABI from pinned host buffers (e2e) ----
-    ri_host = torch.from_numpy(np.ascontiguousarray(real.gv).view(np.float64)).pin_memory()
-    nt_host = torch.from_numpy(np.ascontiguousarray(real.counts)).pin_memory()
-    nclen = real.nclen
-    out_bl = torch.empty((len(tri), nclen, nclen), dtype=torch.float64).pin_memory()
-    out_nt = torch.empty((len(tri), nclen, nclen), dtype=torch.float64).pin_memory()
-    h2d = ri_host.numel() * 8 + nt_host.numel() * 8
-    d2h = out_bl.numel() * 8 + out_nt.numel() * 8 + rdata.size * 8
-
-    def e2e_step():
-        est.load_grid_raw(ri_host.data_ptr(), nt_host.data_ptr(), real.nn, real.nc, real.du, real.flag_key)
-        est.set_rings(real.ulow, real.uhigh)
-        est.set_channels(real.nc10, real.uf_chans)
-        rd = est.calcr()
-        est.run(rd[:, :3].astype(np.int32) if not args.tri_subset else tri, want_v2=True)
-        est.fetch_into(out_bl.data_ptr(), out_nt.data_ptr())
-        return est.last_run_stats()[0]
-
-    for _ in range(max(1, args.warmup - 1)):
-        e2e_step()
+    # ---- end to end through the public API from host memory (e2e) ----
+    run_batch(eng, reals, batches[0])  # warm-up of the host-input path
     barrier()
-    lat = []
+    h2d = d2h = 0
+    path_diff, counts_equal = 0.0, True
     f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    q0 = eng.stats()
     f0.record(stream)
-    e2e_products = 0.0
-    for _ in range(args.steps):
+    lat = []
+    for idx in order:
         t0 = time.perf_counter()
-        e2e_products += e2e_step()
+        res = run_batch(eng, reals, idx)
         lat.append(time.perf_counter() - t0)
+        for i, r in zip(idx, res):
+            h2d += reals[i].gv.nbytes + reals[i].counts.size * 8
+            d2h += sum(a.nbytes for a in r[:4] if a is not None)
+            # the host-input path computes what the device-resident path did (to FP64 rounding: the
+            # engine may group the realisations into other launches)
+            for a, b in ((r[1], mixed[i][1]), (r[3], mixed[i][3])):
+                path_diff = max(path_diff, float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)))
+            counts_equal = counts_equal and np.array_equal(r[2], mixed[i][2])
     f1.record(stream)
     barrier()
-    e2e_ms = max_over_ranks(f0.elapsed_time(f1))
-    e2e_value = sum_over_ranks(e2e_products) / (e2e_ms * 1e-3)
+    q1 = eng.stats()
+    e2e_ms = reduce(f0.elapsed_time(f1), dist.ReduceOp.MAX if world > 1 else None)
+    e2e_value = reduce(q1["products"] - q0["products"], dist.ReduceOp.SUM if world > 1 else None) / (e2e_ms * 1e-3)
+    est.close()
 
-    # ---- plain FP64 GPU path and the mixed path's error on a bounded sample ----
-    fp64 = None
-    if rank == 0 and not args.no_fp64:
-        sample = tri[-3:]  # the three triangles with the largest map (r1 = 15, Ng1 = 740)
-        est.run(sample, want_v2=True)
-        mixed_bl, _, mixed_nt = est.fetch(want_v2=True)
-        p_mixed, ms_mixed = est.last_run_stats()
-        res = {}
-        for prec in ("fp64", "fp64_abs"):
-            with amber_b200.Estimator(device=local, precision=prec, stream=stream.cuda_stream) as e64:
-                e64.load_grid(real.gv, real.counts, real.du, real.flag_key)
-                e64.set_rings(real.ulow, real.uhigh)
-                e64.set_channels(real.nc10, real.uf_chans)
-                e64.run(sample, want_v2=True)
-                res[prec] = (e64.fetch(want_v2=True), e64.last_run_stats())
-        (bl64, _, nt64), (p64, ms64) = res["fp64"]
-        (ab_bl, _, ab_nt), _ = res["fp64_abs"]
-        err = max(float((np.abs(mixed_bl - bl64) / (ab_bl + 1e-300)).max()),
-                  float((np.abs(mixed_nt - nt64) / (ab_nt + 1e-300)).max()))
-        fp64 = {"value": p64 / (ms64 * 1e-3), "unit": UNIT,
-                "sample": "the 3 triangles with r1=15 (Ng1=740), v2, same GPU",
-                "mixed_same_sample": p_mixed / (ms_mixed * 1e-3), "speedup": (p64 / ms64) / (p_mixed / ms_mixed),
-                "max_rel_err_vs_fp64": err, "err_scale": "sum of |products| per lag cell"}
-        fp64["speedup"] = fp64["mixed_same_sample"] / fp64["value"]
+    pk, pk_kind = peaks()
+    peak = pk.get("bf16_tflops_sustained", pk.get("bf16_tflops"))
+    per_launch = products / max(launches, 1)
+    avg_launch_ms = kms / max(launches, 1)
+    achieved = 2.0 * per_launch / (avg_launch_ms * 1e-3) / 1e12 if avg_launch_ms > 0 else None
+    # digit MMAs per product: 6 int8 MACs for the D sums (classes 0-2 of 3x3 digits), 9 for the mask
+    # sums (classes 0-3 of 3x4 digits); a v2 run has as many products of each
+    int8_tops = None if achieved is None else achieved * 7.5
+    roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+            "frac": None if achieved is None else achieved / peak,
+            "traffic": None if DRAM_BYTES_PER_PRODUCT is None else DRAM_BYTES_PER_PRODUCT * per_launch,
+            "kernel": "ls_i8_kernel", "launches": int(launches), "avg_launch_ms": avg_launch_ms,
+            "per_launch_products": per_launch,
+            "timing": "CUDA events around every contraction launch (engine phase events), summed",
+            "traffic_source": "ncu dram__bytes_read+write of one launch (profiles/ls_i8_kernel_config2_one_triangle"
+                              ".txt), scaled by products per launch",
+            "peak_kind": f"{pk_kind} bf16 dense, sustained (int8 MMA nominal rate is 2x this)",
+            "int8_digit_mmas": {"macs_per_product": 7.5, "tops": int8_tops,
+                                "frac_of_2x_bf16_peak": None if int8_tops is None else int8_tops / (2 * peak)},
+            "share_of_busy": kms / max(s1["busy_ms"] - s0["busy_ms"], 1e-9)}
 
-    # ---- CPU baseline: the reference's own loop on the host cores ----
-    cpu = None
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "int8 tensor-core digits, int32 accumulate, fp64 reduce",
+           "data": "synthetic (seeded Gaussian fields, Poisson sampling, random flags; per-rank seeds)",
+           "config": dict(WORKLOAD, parallelism=f"replicas x{world}",
+                          l2="inputs larger than L2: every step streams 8 realisations' maps (GBs) through HBM"),
+           "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d / args.steps),
+                   "d2h_bytes_per_step": int(d2h / args.steps),
+                   "p50_ms": 1e3 * float(np.percentile(lat, 50)), "p99_ms": 1e3 * float(np.percentile(lat, 99)),
+                   "path": "amber_cuda_enqueue / amber_cuda_result with host buffers (cube in, lag arrays out)",
+                   "max_rel_diff_vs_device_resident": path_diff, "counts_equal": counts_equal},
+           "roofline": roof, "clocks": clk, "gpu_launches": int(gpu_launches),
+           "products_per_step": products / args.steps, "generation_s": t_gen,
+           "engine": {k: s1[k] - s0[k] for k in ("rounds", "setup_ms", "maps_ms", "contract_ms", "finish_ms")}}
+
+    if rank == 0 and world == 1 and not args.no_fp64:
+        try:
+            out["fp64_plain"] = fp64_section(amber_b200, torch, reals, cubes, local,
+                                             {i: mixed[i] for i in (0, 16, 48) if i in mixed})
+            out["fp64_plain"]["mixed_whole_ensemble"] = value
+            out["fp64_plain"]["speedup"] = value / out["fp64_plain"]["value"]
+        except Exception as ex:  # reported, not fatal
+            out["fp64_plain"] = {"error": str(ex)[:300]}
+    if rank == 0 and world == 1 and not args.no_single:
+        try:
+            out["single_realisation"] = single_section(amber_b200, synth, local, stream)
+        except Exception as ex:
+            out["single_realisation"] = {"error": str(ex)[:300]}
     if rank == 0 and not args.no_cpu_baseline:
         try:
             import oracle
             if oracle.ref_available():
-                st, rp = cpu_reference_sample(real)
-                cpu = {"value": st["products"] / st["accum_s"], "unit": UNIT, "cores": st["threads"],
-                       "kind": "reference",
-                       "sample": f"one triangle (rp={rp}, Ng1=740) of this workload, v1 accumulation loop of the "
-                                 f"reference's own sources (oracle/_ref/ref_amber_fast), {st['accum_s']:.1f} s"}
+                st, rp = cpu_reference_sample(reals[CPU_SAMPLE_REALISATION])
+                r = reals[CPU_SAMPLE_REALISATION]
+                out["cpu_baseline"] = {
+                    "value": st["products"] / st["accum_s"], "unit": UNIT, "cores": st["threads"], "kind": "reference",
+                    "sample": f"ensemble realisation {CPU_SAMPLE_REALISATION} (side {r.nn}, {r.nc} channels), its last "
+                              f"triangle rp={rp}, v1 accumulation loop of the reference's own sources "
+                              f"(oracle/_ref/ref_amber_fast), {st['accum_s']:.1f} s"}
         except Exception as ex:  # reported, not fatal
-            cpu = {"value": None, "unit": UNIT, "error": str(ex)[:200]}
-
-    pk, pk_kind = peaks()
-    # algorithmic flops of one contraction launch = 2 per product; products per launch = p/(launches)
-    per_launch_products = products / max(contracts, 1)
-    avg_launch_ms = contract_ms / max(contracts, 1)
-    achieved = 2.0 * per_launch_products / (avg_launch_ms * 1e-3) / 1e12
-    peak = pk.get("bf16_tflops_sustained", pk.get("bf16_tflops"))
-    # the digit scheme runs 9 int8 MACs per lag-triple product (3 x 4 digits, classes i+j <= 3)
-    int8_tops = 2.0 * 9 * per_launch_products / (avg_launch_ms * 1e-3) / 1e12
-    roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-            "traffic": DRAM_BYTES_PER_PRODUCT * per_launch_products, "kernel": "contract_i8_kernel",
-            "traffic_source": "ncu dram__bytes_read+write of one launch (profiles/"
-                              "contract_i8_kernel_config2_one_triangle.txt), scaled by products per launch",
-            "peak_kind": f"{pk_kind} bf16 dense, sustained (int8 MMA nominal rate is 2x this)",
-            "int8_digit_mmas": {"macs_per_product": 9, "tops": int8_tops, "frac_of_2x_bf16_peak": int8_tops / (2 * peak)},
-            "per_launch_products": per_launch_products, "avg_launch_ms": avg_launch_ms,
-            "share_of_step": contract_ms / max(sum(step_ms), 1e-9),
-            "phase_ms_per_step": {"maps": maps_ms / args.steps, "contract": contract_ms / args.steps,
-                                  "lag_reduce": reduce_ms / args.steps}}
-    lat_ms = sorted(1e3 * x for x in lat)
-    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-           "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
-           "vs_baseline": None, "dtype": "int8 tensor-core digits, int32 accumulate, fp64 reduce",
-           "data": "synthetic (seeded Gaussian field, Poisson sampling, per-rank seed)",
-           "config": dict(WORKLOAD, parallelism=f"replicas x{world}", l2="256 MB flush between steps; working set "
-                                                                          "(maps) > L2"),
-           "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-                   "p50_ms": float(np.percentile(lat_ms, 50)), "p99_ms": float(np.percentile(lat_ms, 99))},
-           "fp64_plain": fp64, "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
-           "gpu_launches": int(launches), "products_per_step": products / args.steps}
-    out["autotuner"] = {f"nclen<={k}": {"tile_n": v[0], "trial_ms_32": round(v[1], 3), "trial_ms_64": round(v[2], 3)}
-                        for k, v in est.tile_choices().items()}
-    est.close()
-    # batched ensemble and serving stream: 1 GPU only (the scaling runs measure the step above)
-    if rank == 0 and world == 1 and not args.tri_subset:
-        for key, flag, fn in (("ensemble", args.no_ensemble, ensemble_section),
-                              ("serving", args.no_serving, serving_section)):
-            if flag:
-                continue
-            try:
-                out[key] = fn(amber_b200, synth, local)
-            except Exception as ex:  # reported, not fatal
-                out[key] = {"error": str(ex)[:300]}
+            out["cpu_baseline"] = {"value": None, "unit": UNIT, "error": str(ex)[:200]}
+    del keep
     if rank == 0:
         print(json.dumps(out))
     if world > 1:
