@@ -343,6 +343,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         const bool row_ok = r < mrows;
         const uint32_t lane_field = (uint32_t)(32 * q) << 16;
         const int ngr = g1 - g0, nab1 = c1 - c0;
+        const int row0_3 = c0 - jd->nc10 + (ks > 1 ? 0 : LS_ROWS * u.t3);  // channel of staged D3 row 0
         int ns = 0, na = 0, ni = 0;
         // One iteration fills the A buffers of two anchor groups (one barrier round trip, one
         // tcgen05.wait::st).  A lane whose row has no data (past the tile or past the anchor
@@ -367,7 +368,10 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                     const int p1 = sgroups[gi + h] + a;
                     const int rho = p1 - c0 + d3;  // staged D3 row of this lane
                     const bool valid = row_ok && p1 < c1;
-                    if (__any_sync(0xffffffffu, valid)) {
+                    const int p3 = row0_3 + rho;  // D3 channel of this lane's row
+                    // a warp whose rows all fall outside [0, nc) (zero rows of the TMA bounds fill)
+                    // stores zero digits without the arithmetic
+                    if (__any_sync(0xffffffffu, valid && p3 >= 0 && p3 < nc)) {
                         const unsigned char *row3 = valid ? st + ST_D3 + rho * 128 : zero_row;
                         const float4 x0 = *reinterpret_cast<const float4 *>(row3 + (((2 * ps) ^ (rho & 7)) << 4));
                         const float4 x1 = *reinterpret_cast<const float4 *>(row3 + (((2 * ps + 1) ^ (rho & 7)) << 4));
