@@ -70,7 +70,8 @@ constexpr int WARP_TMA = 16, WARP_MMA = 17;
 constexpr int NTHREADS = 18 * 32;
 constexpr int TMEM_COLS = 512;
 constexpr int ACC_STRIDE = 128;              // TMEM columns per class accumulator
-constexpr int NABUF = 4;                     // A buffers
+constexpr int NABUF = 5;                     // A buffers
+constexpr int NSET = 4;                      // former sets: each anchor group is formed by one set of 4 warps
 constexpr int ABUF_COLS = 24;                // 3 digits × 8 columns (32 int8 per row per digit)
 constexpr int A_COL0 = 3 * ACC_STRIDE;       // first A buffer column
 static_assert(A_COL0 + NABUF * ABUF_COLS <= TMEM_COLS, "TMEM");
@@ -128,9 +129,11 @@ __device__ __forceinline__ uint32_t pack_low_bytes(float a, float b, float c, fl
                        __byte_perm(__float_as_uint(c), __float_as_uint(d), 0x0040), 0x5410);
 }
 
-__device__ __forceinline__ void tmem_st2(uint32_t taddr, uint32_t a, uint32_t b)
+__device__ __forceinline__ void tmem_st4(uint32_t taddr, const uint32_t (&v)[4])
 {
-    asm volatile("tcgen05.st.sync.aligned.32x32b.x2.b32 [%0], {%1, %2};" ::"r"(taddr), "r"(a), "r"(b) : "memory");
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1, %2, %3, %4};" ::"r"(taddr), "r"(v[0]), "r"(v[1]),
+                 "r"(v[2]), "r"(v[3])
+                 : "memory");
 }
 
 __device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&v)[8])
@@ -225,7 +228,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     if (tid < 32) reinterpret_cast<uint32_t *>(zero_row)[tid] = 0u;
     if (tid == 0) {
         for (int s = 0; s < NSTAGE; ++s) { mbar_init(&st_full[s], 1); mbar_init(&st_empty[s], NFORM + 1); }
-        for (int s = 0; s < NABUF; ++s) { mbar_init(&ab_full[s], NFORM); mbar_init(&ab_empty[s], 1); }
+        for (int s = 0; s < NABUF; ++s) { mbar_init(&ab_full[s], NFORM / NSET); mbar_init(&ab_empty[s], 1); }
         mbar_init(acc_full, 1);
         mbar_init(acc_empty, NFORM);
         mbar_init(drain, 1);
@@ -345,68 +348,81 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         const int ngr = g1 - g0, nab1 = c1 - c0;
         const int row0_3 = c0 - jd->nc10 + (ks > 1 ? 0 : LS_ROWS * u.t3);  // channel of staged D3 row 0
         int ns = 0, na = 0, ni = 0;
-        // One iteration fills the A buffers of two anchor groups (one barrier round trip, one
-        // tcgen05.wait::st).  A lane whose row has no data (past the tile or past the anchor
-        // block) reads a zeroed row, so its digits come out zero with no per-digit select; D3
-        // channels outside [0, nc) arrive as zero rows from the TMA bounds fill.  A warp with no
-        // such lane skips the arithmetic.
+        // The 16 formers are four sets of four: set ps forms anchor groups ps, ps + 4, … of each
+        // slice, and within a set warp q fills TMEM lanes 32q .. 32q+31 of the group's A buffer
+        // with all 32 pixels (four 8-pixel chunks, one tcgen05.st.x8 per digit plane), so the
+        // per-group work (addresses, barrier wait, TMEM hand-off) is spread over 32 pixels.  A
+        // lane whose row has no data (past the tile or past the anchor block) reads a zeroed row,
+        // so its digits come out zero with no per-digit select; D3 channels outside [0, nc) arrive
+        // as zero rows from the TMA bounds fill, and a warp whose rows all lie there stores zero
+        // digits without the arithmetic.
         auto form_slice = [&](auto ndc, const unsigned char *st) {
             constexpr int ND = decltype(ndc)::value;
-            for (int gi = 0; gi < ngr && ok; gi += 2) {
-                const int nb2 = min(2, ngr - gi);
-                for (int h = 0; h < nb2; ++h)
-                    if (!mbar_wait_warp(&ab_empty[(na + h) % NABUF], (((na + h) / NABUF) & 1) ^ 1, abort_flag, err,
-                                        36)) {
-                        ok = false;
-                        break;
-                    }
-                if (!ok) break;
-                uint32_t w[2][3][2];
+            constexpr int D0 = ND - 3;  // sweep 2 stores product digits 1-3
+            for (int g = ps; g < ngr && ok; g += NSET) {
+                const int n = na + g;  // the group's place in the MMA warp's order
+                if (!mbar_wait_warp(&ab_empty[n % NABUF], ((n / NABUF) & 1) ^ 1, abort_flag, err, 36)) {
+                    ok = false;
+                    break;
+                }
+                const int p1 = sgroups[g] + a;
+                const int rho = p1 - c0 + d3;  // staged D3 row of this lane
+                const bool valid = row_ok && p1 < c1;
+                const int p3 = row0_3 + rho;  // D3 channel of this lane's row
+                // two halves of 16 pixels: 12 digit words stay live until their tcgen05.wait::st
+                // (the 18 warps leave ~96 registers a thread)
+                const bool live = __any_sync(0xffffffffu, valid && p3 >= 0 && p3 < nc);
+                const unsigned char *row3 = valid ? st + ST_D3 + rho * 128 : zero_row;
+                // the D1 row, already scaled by 127·2^−(E1+E3) for this block
+                const float4 *row1 = reinterpret_cast<const float4 *>(st + ST_D1 + min(p1 - c0, nab1 - 1) * 128);
+                const uint32_t col = tmem + lane_field + A_COL0 + (n % NABUF) * ABUF_COLS;
 #pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    if (h >= nb2) break;
-                    const int p1 = sgroups[gi + h] + a;
-                    const int rho = p1 - c0 + d3;  // staged D3 row of this lane
-                    const bool valid = row_ok && p1 < c1;
-                    const int p3 = row0_3 + rho;  // D3 channel of this lane's row
-                    // a warp whose rows all fall outside [0, nc) (zero rows of the TMA bounds fill)
-                    // stores zero digits without the arithmetic
-                    if (__any_sync(0xffffffffu, valid && p3 >= 0 && p3 < nc)) {
-                        const unsigned char *row3 = valid ? st + ST_D3 + rho * 128 : zero_row;
-                        const float4 x0 = *reinterpret_cast<const float4 *>(row3 + (((2 * ps) ^ (rho & 7)) << 4));
-                        const float4 x1 = *reinterpret_cast<const float4 *>(row3 + (((2 * ps + 1) ^ (rho & 7)) << 4));
-                        // the D1 row, already scaled by 127·2^−(E1+E3) for this block
-                        const float4 *row1 =
-                            reinterpret_cast<const float4 *>(st + ST_D1 + min(p1 - c0, nab1 - 1) * 128 + 32 * ps);
-                        const float4 u0 = row1[0], u1 = row1[1];
-                        float2 ya[4], yb[4], yc[4], yd[4];
-                        digits254x2<ND>(make_float2(u0.x, u0.y), make_float2(x0.x, x0.y), ya);
-                        digits254x2<ND>(make_float2(u0.z, u0.w), make_float2(x0.z, x0.w), yb);
-                        digits254x2<ND>(make_float2(u1.x, u1.y), make_float2(x1.x, x1.y), yc);
-                        digits254x2<ND>(make_float2(u1.z, u1.w), make_float2(x1.z, x1.w), yd);
-                        constexpr int D0 = ND - 3;  // sweep 2 stores product digits 1-3
+                for (int half = 0; half < 2; ++half) {
+                    uint32_t w[3][4];
+                    if (live) {
 #pragma unroll
-                        for (int dd = 0; dd < 3; ++dd) {
-                            w[h][dd][0] = pack_low_bytes(ya[dd + D0].x, ya[dd + D0].y, yb[dd + D0].x, yb[dd + D0].y);
-                            w[h][dd][1] = pack_low_bytes(yc[dd + D0].x, yc[dd + D0].y, yd[dd + D0].x, yd[dd + D0].y);
+                        for (int cc = 0; cc < 2; ++cc) {
+                            const int c = 2 * half + cc;
+                            const float4 x0 = *reinterpret_cast<const float4 *>(row3 + (((2 * c) ^ (rho & 7)) << 4));
+                            const float4 x1 =
+                                *reinterpret_cast<const float4 *>(row3 + (((2 * c + 1) ^ (rho & 7)) << 4));
+                            const float4 u0 = row1[2 * c], u1 = row1[2 * c + 1];
+                            {  // pixels 0-3 of the chunk -> word 2cc of each digit plane
+                                float2 ya[4], yb[4];
+                                digits254x2<ND>(make_float2(u0.x, u0.y), make_float2(x0.x, x0.y), ya);
+                                digits254x2<ND>(make_float2(u0.z, u0.w), make_float2(x0.z, x0.w), yb);
+#pragma unroll
+                                for (int dd = 0; dd < 3; ++dd)
+                                    w[dd][2 * cc] =
+                                        pack_low_bytes(ya[dd + D0].x, ya[dd + D0].y, yb[dd + D0].x, yb[dd + D0].y);
+                            }
+                            {  // pixels 4-7 -> word 2cc + 1
+                                float2 yc[4], yd[4];
+                                digits254x2<ND>(make_float2(u1.x, u1.y), make_float2(x1.x, x1.y), yc);
+                                digits254x2<ND>(make_float2(u1.z, u1.w), make_float2(x1.z, x1.w), yd);
+#pragma unroll
+                                for (int dd = 0; dd < 3; ++dd)
+                                    w[dd][2 * cc + 1] =
+                                        pack_low_bytes(yc[dd + D0].x, yc[dd + D0].y, yd[dd + D0].x, yd[dd + D0].y);
+                            }
                         }
                     } else {
 #pragma unroll
-                        for (int dd = 0; dd < 3; ++dd) w[h][dd][0] = w[h][dd][1] = 0u;
-                    }
-                    // pixels 8ps .. 8ps+7 of the slice = columns 2ps, 2ps+1 of each digit's 8
-                    const uint32_t col = tmem + lane_field + A_COL0 + ((na + h) % NABUF) * ABUF_COLS + 2 * ps;
+                        for (int dd = 0; dd < 3; ++dd)
 #pragma unroll
-                    for (int dd = 0; dd < 3; ++dd) tmem_st2(col + 8 * dd, w[h][dd][0], w[h][dd][1]);
+                            for (int e = 0; e < 4; ++e) w[dd][e] = 0u;
+                    }
+                    // pixels 16·half .. +15 = columns 4·half .. +3 of each digit plane
+#pragma unroll
+                    for (int dd = 0; dd < 3; ++dd) tmem_st4(col + 8 * dd + 4 * half, w[dd]);
+                    // tcgen05.st reads its source registers asynchronously: wait before they change
+                    asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
                 }
-                // tcgen05.st reads its source registers asynchronously: wait before they change
-                asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
                 fence_before();
                 __syncwarp();
-                if (lane == 0)
-                    for (int h = 0; h < nb2; ++h) mbar_arrive(&ab_full[(na + h) % NABUF]);
-                na += nb2;
+                if (lane == 0) mbar_arrive(&ab_full[n % NABUF]);
             }
+            na += ngr;
         };
         for (long b = u.b0; b < u.b1 && ok; ++b) {
             const int E13 = jd->e1[b] + jd->e3[b];
