@@ -10,11 +10,15 @@
  * i32 numdnu[nclen²]} (amber.c:287-304), v2 bsout_final2_… = {f64 1/Ng1²,
  * f32 bldnu, f32 numdnu} (amber_v2.c:295-309).  The constants the reference
  * hard-codes (amber.c:43-54,187 and the ring edges of annular_rings) are
- * arguments here.  Errors keep the reference's behaviour: perror/fprintf + exit.
+ * optional arguments here whose defaults are the reference's own: v1, nc10 =
+ * 383 (amber.c:46) and the 22 annular_rings edges (amber_funcs.c:2022-2062,
+ * amber.c:44-45), so `amber_gpu <Rlzn>` runs what `amber <Rlzn>` runs.  Errors
+ * keep the reference's behaviour: perror/fprintf + exit.
  *
- * usage: amber_gpu <Rlzn> <v1|v2> <nc10> <rings_file> [rp_begin] [rp_end] [res_path]
+ * usage: amber_gpu <Rlzn> [v1|v2] [nc10|-] [rings_file|-] [rp_begin] [rp_end] [res_path]
  *                  [input_params_ess] [mixed|fp64]
- * rings_file: "Nr" then Nr lines "ULow UHigh".
+ *        amber_gpu --default-rings      (print the default ring edges and exit)
+ * rings_file: "Nr" then Nr lines "ULow UHigh"; "-" keeps the default.
  */
 #include <errno.h>
 #include <stdint.h>
@@ -39,18 +43,44 @@ static void check(amber_cuda_ctx *ctx, int rc, const char *what)
     }
 }
 
+/* The reference's ring edges (annular_rings, amber_funcs.c:2022-2062): lower edges on a
+ * piecewise-uniform ladder, 0-50 in steps of 5, 50-100 in 10, 100-200 in 20, 200-270 in 35,
+ * each ring's upper edge the next ring's lower one, then the first lower edge raised to 1
+ * and the last upper edge set to 270.  DEFAULT_NR = 22 is the bin count of amber.c:44-45. */
+#define DEFAULT_NR 22
+static void default_rings(double *ulow, double *uhigh)
+{
+    static const int ladder[4][3] = {{0, 50, 5}, {50, 100, 10}, {100, 200, 20}, {200, 270, 35}};
+    int n = 0;
+    for (int k = 0; k < 4; ++k)
+        for (int e = ladder[k][0]; e < ladder[k][1] && n < DEFAULT_NR; e += ladder[k][2]) {
+            ulow[n] = e;
+            if (n > 0) uhigh[n - 1] = e;
+            ++n;
+        }
+    ulow[0] = 1.0;
+    uhigh[DEFAULT_NR - 1] = 270.0;
+}
+
 int main(int argc, char **argv)
 {
-    if (argc < 5) {
-        printf("Usage: %s <Rlzn> <v1|v2> <nc10> <rings_file> [rp_begin] [rp_end] [res_path] [input_params_ess] "
+    if (argc == 2 && strcmp(argv[1], "--default-rings") == 0) {
+        double lo[DEFAULT_NR], hi[DEFAULT_NR];
+        default_rings(lo, hi);
+        printf("%d\n", DEFAULT_NR);
+        for (int i = 0; i < DEFAULT_NR; ++i) printf("%.17g %.17g\n", lo[i], hi[i]);
+        return 0;
+    }
+    if (argc < 2) {
+        printf("Usage: %s <Rlzn> [v1|v2] [nc10|-] [rings_file|-] [rp_begin] [rp_end] [res_path] [input_params_ess] "
                "[mixed|fp64]\n",
                argv[0]);
         return 1;
     }
     const int rlzn = atoi(argv[1]);
-    const int v2 = strcmp(argv[2], "v2") == 0;
-    const int nc10 = atoi(argv[3]);
-    const char *rings_file = argv[4];
+    const int v2 = argc > 2 && strcmp(argv[2], "v2") == 0;
+    const int nc10 = (argc > 3 && strcmp(argv[3], "-") != 0) ? atoi(argv[3]) : 383;  /* amber.c:46 */
+    const char *rings_file = (argc > 4 && strcmp(argv[4], "-") != 0) ? argv[4] : NULL;
     int rp_begin = argc > 5 ? atoi(argv[5]) : 0;
     int rp_end = argc > 6 ? atoi(argv[6]) : -1;
     const char *res_path = argc > 7 ? argv[7] : (v2 ? "results/v2" : "results/v1");
@@ -99,21 +129,31 @@ int main(int argc, char **argv)
     }
     fclose(fp);
 
-    /* rings */
-    fp = fopen(rings_file, "r");
-    if (!fp) die("Error opening rings file");
-    int Nr;
-    if (fscanf(fp, "%d", &Nr) != 1 || Nr <= 0) {
-        fprintf(stderr, "rings file: bad count\n");
-        exit(EXIT_FAILURE);
-    }
-    double *ulow = (double *)malloc(sizeof(double) * Nr), *uhigh = (double *)malloc(sizeof(double) * Nr);
-    for (int i = 0; i < Nr; ++i)
-        if (fscanf(fp, "%lf %lf", &ulow[i], &uhigh[i]) != 2) {
-            fprintf(stderr, "rings file: bad edges\n");
+    /* rings: the file's, or the reference's own edges */
+    int Nr = DEFAULT_NR;
+    double *ulow, *uhigh;
+    if (rings_file) {
+        fp = fopen(rings_file, "r");
+        if (!fp) die("Error opening rings file");
+        if (fscanf(fp, "%d", &Nr) != 1 || Nr <= 0) {
+            fprintf(stderr, "rings file: bad count\n");
             exit(EXIT_FAILURE);
         }
-    fclose(fp);
+        ulow = (double *)malloc(sizeof(double) * Nr);
+        uhigh = (double *)malloc(sizeof(double) * Nr);
+        if (!ulow || !uhigh) die("malloc");
+        for (int i = 0; i < Nr; ++i)
+            if (fscanf(fp, "%lf %lf", &ulow[i], &uhigh[i]) != 2) {
+                fprintf(stderr, "rings file: bad edges\n");
+                exit(EXIT_FAILURE);
+            }
+        fclose(fp);
+    } else {
+        ulow = (double *)malloc(sizeof(double) * Nr);
+        uhigh = (double *)malloc(sizeof(double) * Nr);
+        if (!ulow || !uhigh) die("malloc");
+        default_rings(ulow, uhigh);
+    }
 
     /* uf_chans.txt when the data are flagged: one integer per unflagged channel */
     int uf_nc = 0;

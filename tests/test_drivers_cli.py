@@ -41,6 +41,30 @@ def test_vcg_rejects_more_channels_than_the_file_holds(exes, tmp_path):
     assert p.returncode == 1 and "holds 3" in p.stderr
 
 
+def test_amber_gpu_runs_on_the_reference_defaults(exes, tmp_path):
+    """`amber_gpu <Rlzn>` alone, as `amber <Rlzn>` is run: the version, nc10 and rings default to the
+    reference's (v1, nc10 = 383, the annular_rings edges), so it goes straight to its inputs."""
+    p = _run([exes.DRIVER], tmp_path)
+    assert p.returncode == 1 and "Usage" in p.stdout
+    p = _run([exes.DRIVER, "1"], tmp_path)
+    assert p.returncode != 0 and "input_params_ess" in p.stderr
+
+
+def test_amber_gpu_default_rings_are_the_reference_annular_rings(exes):
+    """The driver's default ring edges equal those the reference's own annular_rings() sets
+    (4_fbe/amber_funcs.c:2022-2062 compiled unchanged into oracle/_ref/ref_rings), for the 22 bins
+    of amber.c:44-45, digit for digit."""
+    import oracle
+    ref = os.path.join(oracle.REF_DIR, "ref_rings")
+    if not os.path.exists(ref):
+        pytest.skip("reference build oracle/_ref missing (make -C oracle ref)")
+    ours = subprocess.run([exes.DRIVER, "--default-rings"], capture_output=True, text=True, check=True).stdout
+    theirs = subprocess.run([ref], capture_output=True, text=True, check=True).stdout
+    assert ours == theirs
+    lines = ours.split("\n")
+    assert lines[0] == "22" and lines[1] == "1 5" and lines[22] == "235 270"
+
+
 def test_maps_usage_and_missing_inputs(exes, tmp_path):
     p = _run([exes.MAPS_DRIVER], tmp_path)
     assert p.returncode == 1 and "Usage" in p.stdout
