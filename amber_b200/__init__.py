@@ -177,9 +177,9 @@ class Estimator:
     precision: "mixed" (int8 tensor-core digits, ≤1e-6 of Σ|products| per lag cell), "fp64"
     (plain FP64, ≤1e-10), "fp64_abs" (FP64 over |maps|: the error scale) or "bf16x3"
     (comparison only).  hbm_budget: bytes the context may hold (0: most of the free memory).
-    stream: a cudaStream_t to launch on.  chunk_px: pixels per accumulation chunk (0: planned).
-    tile_n: the contraction's p3 tile width, 32, 64 or 128 (0: the autotuner's choice); results
-    do not depend on it.  Every call raises AmberError with the library's message on failure.
+    stream: a cudaStream_t to launch on.  chunk_px: pixels per contraction work unit, i.e. per
+    FP64 partial lag tile, rounded up to 256-pixel blocks (0: planned); it sets only the summation grouping.
+    tile_n: accepted for compatibility and ignored (the lag-space contraction has no tile width).  Every call raises AmberError with the library's message on failure.
     """
 
     def __init__(self, device: int = 0, precision: str = "mixed", hbm_budget: int = 0, stream: int | None = None,
@@ -365,8 +365,8 @@ class Estimator:
         return out[:ntri]
 
     def tile_choices(self) -> dict:
-        """Autotuner decisions: {nclen class: (tile width, trial ms at 32, at 64)} (0 when another context
-        of the process ran the trial)."""
+        """Kept for compatibility with the earlier tile-width autotuner: the lag-space contraction has no
+        tile width to choose, so this is empty."""
         n = self._L.amber_cuda_tile_choices(self._h, 0, None, None, None, None)
         cls, bn = np.zeros(max(n, 1), np.int32), np.zeros(max(n, 1), np.int32)
         t32, t64 = np.zeros(max(n, 1), np.float32), np.zeros(max(n, 1), np.float32)

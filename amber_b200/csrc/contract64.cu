@@ -301,7 +301,7 @@ int contract_fp64_jobs(amber_cuda_ctx *c, const std::vector<F64Job> &jobs)
         size_t j1 = j0;
         for (; j1 < jobs.size(); ++j1) {
             LsJobPlan p;
-            ls_plan_job(p, (int)c->nc, c->nc10, jobs[j1].k, c->weight, c->num_sms);
+            ls_plan_job(p, (int)c->nc, c->nc10, jobs[j1].k, c->weight, c->num_sms, 8, ls_force_bpu(c->chunk_px));
             if (j1 > j0 && (size_t)(tiles + p.s.units()) * TILE_B > pcap) break;
             p.unit_base = tiles;
             tiles += p.s.units();

@@ -536,7 +536,7 @@ int contract_i8_jobs(amber_cuda_ctx *c, const std::vector<I8Job> &jobs)
         for (; j1 < jobs.size(); ++j1) {
             const I8Job &jb = jobs[j1];
             LsJobPlan p;
-            ls_plan_job(p, jb.nc, jb.nc10, jb.k, *jb.weight, c->num_sms);
+            ls_plan_job(p, jb.nc, jb.nc10, jb.k, *jb.weight, c->num_sms, 8, ls_force_bpu(c->chunk_px));
             if (j1 > j0 && (size_t)(tiles + p.s.units()) * TILE_B > pcap) break;
             p.unit_base = tiles;
             tiles += p.s.units();

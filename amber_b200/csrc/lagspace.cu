@@ -49,7 +49,7 @@ int LsShape::cols(int t2) const
 }
 int LsShape::lag_cols(int t2) const { return k > 1 ? nclen : std::min(LS_ROWS, nclen - LS_ROWS * t2); }
 
-LsShape ls_shape(int nc, int nc10, long k_px, int sms, long min_bpu)
+LsShape ls_shape(int nc, int nc10, long k_px, int sms, long min_bpu, long force_bpu)
 {
     LsShape s;
     s.nc = nc;
@@ -69,14 +69,16 @@ LsShape ls_shape(int nc, int nc10, long k_px, int sms, long min_bpu)
     // each (a unit's partial tile costs a write and a read of 128 KB).
     const long combos = (long)s.T * s.T * s.nab;
     const long target = 6L * std::max(1, sms);
-    s.bpu = std::min(s.nblk, std::max(min_bpu, (s.nblk * combos + target - 1) / target));
+    s.bpu = force_bpu > 0 ? std::min(s.nblk, force_bpu)
+                          : std::min(s.nblk, std::max(min_bpu, (s.nblk * combos + target - 1) / target));
     s.V = (int)((s.nblk + s.bpu - 1) / s.bpu);
     return s;
 }
 
-void ls_plan_job(LsJobPlan &p, int nc, int nc10, long k_px, const std::vector<int> &weight, int sms, long min_bpu)
+void ls_plan_job(LsJobPlan &p, int nc, int nc10, long k_px, const std::vector<int> &weight, int sms, long min_bpu,
+                 long force_bpu)
 {
-    p.s = ls_shape(nc, nc10, k_px, sms, min_bpu);
+    p.s = ls_shape(nc, nc10, k_px, sms, min_bpu, force_bpu);
     p.groups.clear();
     p.group_off.assign(1, 0);
     for (int ab = 0; ab < p.s.nab; ++ab) {

@@ -55,8 +55,12 @@ struct LsShape {
     int units() const { return T * T * nab * V; }
 };
 
-// min_bpu: fewest pixel blocks per unit (partial-tile traffic against work per unit)
-LsShape ls_shape(int nc, int nc10, long k_px, int sms, long min_bpu = 8);
+// min_bpu: fewest pixel blocks per unit (partial-tile traffic against work per unit);
+// force_bpu > 0: exactly that many blocks per unit (the last unit of a job may hold fewer)
+LsShape ls_shape(int nc, int nc10, long k_px, int sms, long min_bpu = 8, long force_bpu = 0);
+
+// Blocks per unit that a chunk_px option asks for (0 = chosen by the planner)
+inline long ls_force_bpu(int chunk_px) { return chunk_px > 0 ? (chunk_px + LS_BLOCK - 1) / LS_BLOCK : 0; }
 
 // One unit as the kernels see it.
 struct LsUnit {
@@ -77,7 +81,7 @@ struct LsJobPlan {
     long unit_base = 0;           // first partial tile of the job in its launch
 };
 void ls_plan_job(LsJobPlan &p, int nc, int nc10, long k_px, const std::vector<int> &weight, int sms,
-                 long min_bpu = 8);
+                 long min_bpu = 8, long force_bpu = 0);
 void ls_units(const LsJobPlan &p, int job, std::vector<LsUnit> &out);
 
 // Device description of one job for ls_reduce.

@@ -53,10 +53,11 @@ typedef struct amber_cuda_opts {
     int precision;         /* AMBER_PREC_FP64 or AMBER_PREC_MIXED */
     size_t hbm_budget;     /* max device bytes the context may hold; 0 = 90 % of free memory */
     void *stream;          /* optional cudaStream_t to launch on (NULL = the context's own stream) */
-    int chunk_px;          /* tensor-core paths: pixels per CTA accumulation chunk before the FP64 flush (0 = default) */
-    int tile_n;            /* mixed path: p3 tile width 32, 64 or 128 (128: both MMA operands from shared
-                              memory, N = 128); 0 = chosen by the autotuner (measured once per lag-window
-                              class and context).  Results do not depend on it. */
+    int chunk_px;          /* lag-space contraction (mixed and FP64): pixels per work unit, i.e. per partial
+                              lag tile summed in FP64, rounded up to whole 256-pixel blocks; 0 = chosen by the
+                              planner (about six units per SM).  It sets only the FP64 summation grouping. */
+    int tile_n;            /* accepted for compatibility (0, 32, 64 or 128) and ignored: the lag-space
+                              contraction has no tile width to choose */
 } amber_cuda_opts;
 
 AMBER_API void amber_cuda_default_opts(amber_cuda_opts *opts);
@@ -184,11 +185,8 @@ typedef struct amber_cuda_cylbs_params {
 AMBER_API int amber_cuda_cyl_bs(amber_cuda_ctx *ctx, const amber_cuda_cylbs_params *p, const double *tri_div,
                                 double *out);
 
-/* The autotuner's decisions seen by this context (mixed path, tile_n = 0): for each
- * lag-window class (nclen rounded up to 8) the chosen p3 tile width and, where this
- * context ran the trial, the two trials' times in ms (the first pixel chunk of one job,
- * each width alone; decisions are shared by all contexts of the process on a device).
- * Returns the number of classes (entries beyond max_entries are counted, not written).
+/* Kept for compatibility with callers of the earlier tile-width autotuner: the lag-space
+ * contraction has no tile width to choose, so this returns 0 (no entries written).
  * No reference counterpart. */
 AMBER_API int amber_cuda_tile_choices(const amber_cuda_ctx *ctx, int max_entries, int *nclen_class, int *tile_n,
                                       float *ms_trial_32, float *ms_trial_64);
