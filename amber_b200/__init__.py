@@ -40,6 +40,7 @@ EXPORTS = (
     "amber_cuda_last_run_stats", "amber_cuda_last_run_breakdown", "amber_cuda_last_run_shape", "amber_cuda_grid_vis",
     "amber_cuda_enqueue", "amber_cuda_wait", "amber_cuda_result", "amber_cuda_engine_stats",
     "amber_cuda_tile_choices", "amber_cuda_cyl_bs", "amber_cuda_grid_vis_collapsed", "amber_cuda_cl_dnu",
+    "amber_cuda_shard_plan",
 )
 
 

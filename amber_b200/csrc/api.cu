@@ -10,6 +10,7 @@
 
 #include <algorithm>
 #include <set>
+#include <map>
 #include <vector>
 
 #include "lagspace.cuh"
@@ -747,6 +748,53 @@ int amber_cuda_triangles(amber_cuda_ctx *c, int ntri, const int *tri, int want_v
     int rc = amber_cuda_triangles_run(c, ntri, tri, want_v2);
     if (rc) return rc;
     return amber_cuda_triangles_fetch(c, bldnu, numdnu, numtri);
+}
+
+int amber_cuda_shard_plan(int ntri, const int *r1, const long *ng1, int world, int *rank_of)
+{
+    if (ntri < 0 || world < 1 || (ntri > 0 && (!r1 || !ng1 || !rank_of))) return AMBER_ERR_ARG;
+    // r1 groups in ascending r1, each holding its triangles in ascending index
+    std::map<int, std::vector<int>> groups;
+    std::map<int, long long> cost1;
+    for (int t = 0; t < ntri; ++t) {
+        if (ng1[t] <= 0) return AMBER_ERR_ARG;
+        groups[r1[t]].push_back(t);
+        cost1[r1[t]] = (long long)ng1[t] * ng1[t];
+    }
+    long long total = 0;
+    for (const auto &g : groups) total += (long long)g.second.size() * cost1[g.first];
+    struct Part {
+        long long cost, map_cost;
+        int r1;
+        std::vector<int> tri;
+    };
+    std::vector<Part> parts;
+    for (const auto &g : groups) {
+        const long long n = (long long)g.second.size(), gcost = n * cost1[g.first];
+        const long long m = std::max(1LL, std::min(n, (gcost * world + total - 1) / std::max(total, 1LL)));
+        for (long long j = 0; j < m; ++j) {
+            Part p;
+            p.r1 = g.first;
+            for (long long i = j; i < n; i += m) p.tri.push_back(g.second[(size_t)i]);
+            p.cost = (long long)p.tri.size() * cost1[g.first];
+            p.map_cost = gcost;  // in units of 1/25: the group's map building
+            parts.push_back(std::move(p));
+        }
+    }
+    std::stable_sort(parts.begin(), parts.end(), [](const Part &a, const Part &b) {
+        if (a.cost != b.cost) return a.cost > b.cost;
+        if (a.r1 != b.r1) return a.r1 < b.r1;
+        return a.tri[0] < b.tri[0];
+    });
+    std::vector<long long> load(world, 0);  // 25 × cost + map costs
+    for (const Part &p : parts) {
+        int k = 0;
+        for (int i = 1; i < world; ++i)
+            if (load[i] < load[k]) k = i;
+        for (int t : p.tri) rank_of[t] = k;
+        load[k] += 25 * p.cost + p.map_cost;
+    }
+    return AMBER_OK;
 }
 
 int amber_cuda_tile_choices(const amber_cuda_ctx *c, int max_entries, int *nclen_class, int *tile_n,

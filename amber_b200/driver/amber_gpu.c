@@ -18,6 +18,9 @@
  * usage: amber_gpu <Rlzn> [v1|v2] [nc10|-] [rings_file|-] [rp_begin] [rp_end] [res_path]
  *                  [input_params_ess] [mixed|fp64]
  *        amber_gpu --default-rings      (print the default ring edges and exit)
+ * Under RANK / WORLD_SIZE / LOCAL_RANK (one process per GPU) each process takes its share of
+ * the closed triangles (amber_cuda_shard_plan) on GPU LOCAL_RANK and writes their files; rank 0
+ * also writes closed_rings and rcount.  The files are those of a single-process run.
  * rings_file: "Nr" then Nr lines "ULow UHigh"; "-" keeps the default.
  */
 #include <errno.h>
@@ -177,6 +180,16 @@ int main(int argc, char **argv)
 
     amber_cuda_opts opts;
     amber_cuda_default_opts(&opts);
+    /* one process per GPU under a launcher that sets RANK / WORLD_SIZE / LOCAL_RANK (torchrun,
+     * mpirun wrappers): this process's GPU, and its share of the closed triangles below */
+    const char *env_rank = getenv("RANK"), *env_world = getenv("WORLD_SIZE"), *env_local = getenv("LOCAL_RANK");
+    const int world = env_world ? atoi(env_world) : 1;
+    const int rank = (world > 1 && env_rank) ? atoi(env_rank) : 0;
+    if (world < 1 || rank < 0 || rank >= world) {
+        fprintf(stderr, "RANK=%d outside WORLD_SIZE=%d\n", rank, world);
+        exit(EXIT_FAILURE);
+    }
+    if (world > 1 && env_local) opts.device = atoi(env_local);
     opts.precision = precision;
     amber_cuda_ctx *ctx = NULL;
     int rc = amber_cuda_create(&opts, &ctx);
@@ -195,26 +208,49 @@ int main(int argc, char **argv)
     double *rdata = (double *)malloc(sizeof(double) * 4 * (rcount > 0 ? rcount : 1));
     check(ctx, amber_cuda_calcr(ctx, rcount, &rcount, rdata), "calCR");
     mkdir(res_path, 0755);
-    snprintf(path, sizeof(path), "%s/closed_rings", res_path);
-    fp = fopen(path, "wb");
-    if (!fp) die("Error opening file: closed_rings");
-    fwrite(rdata, sizeof(double), 4 * (size_t)rcount, fp);
-    fclose(fp);
-    snprintf(path, sizeof(path), "%s/rcount", res_path);
-    fp = fopen(path, "w");
-    if (!fp) die("Error opening file: rcount");
-    fprintf(fp, "%d", rcount);
-    fclose(fp);
+    if (rank == 0) {  /* the shared files: one writer */
+        snprintf(path, sizeof(path), "%s/closed_rings", res_path);
+        fp = fopen(path, "wb");
+        if (!fp) die("Error opening file: closed_rings");
+        fwrite(rdata, sizeof(double), 4 * (size_t)rcount, fp);
+        fclose(fp);
+        snprintf(path, sizeof(path), "%s/rcount", res_path);
+        fp = fopen(path, "w");
+        if (!fp) die("Error opening file: rcount");
+        fprintf(fp, "%d", rcount);
+        fclose(fp);
+    }
     printf("Total combinations of rings on a plane forming closed triangle = %d\n", rcount);
 
     if (rp_end < 0 || rp_end > rcount) rp_end = rcount;
     if (rp_begin < 0) rp_begin = 0;
-    const int ntri = rp_end > rp_begin ? rp_end - rp_begin : 0;
+    const int nrange = rp_end > rp_begin ? rp_end - rp_begin : 0;
+    /* this process's triangles of the range: all of them, or its share under the shard plan
+     * (amber_cuda_shard_plan: whole triangles, so its files are the single-process ones) */
+    int *rps = (int *)malloc(sizeof(int) * (nrange > 0 ? nrange : 1));
+    int ntri = 0;
+    if (world > 1 && nrange > 0) {
+        int *r1s = (int *)malloc(sizeof(int) * nrange), *owner = (int *)malloc(sizeof(int) * nrange);
+        long *ngs = (long *)malloc(sizeof(long) * nrange);
+        if (!r1s || !owner || !ngs) die("malloc");
+        for (int t = 0; t < nrange; ++t) {
+            r1s[t] = (int)rdata[4 * (rp_begin + t)];
+            ngs[t] = amber_cuda_ng1(ctx, r1s[t]);
+        }
+        check(ctx, amber_cuda_shard_plan(nrange, r1s, ngs, world, owner), "shard plan");
+        for (int t = 0; t < nrange; ++t)
+            if (owner[t] == rank) rps[ntri++] = rp_begin + t;
+        free(r1s);
+        free(owner);
+        free(ngs);
+    } else {
+        for (int t = 0; t < nrange; ++t) rps[ntri++] = rp_begin + t;
+    }
     const int nclen = 2 * nc10 + 1;
     const size_t ncsize = (size_t)nclen * nclen;
     int *tri = (int *)malloc(sizeof(int) * 3 * (ntri > 0 ? ntri : 1));
     for (int t = 0; t < ntri; ++t)
-        for (int j = 0; j < 3; ++j) tri[3 * t + j] = (int)rdata[4 * (rp_begin + t) + j];
+        for (int j = 0; j < 3; ++j) tri[3 * t + j] = (int)rdata[4 * rps[t] + j];
     double *bl = (double *)malloc(sizeof(double) * ncsize * (ntri > 0 ? ntri : 1));
     double *nt = v2 ? (double *)malloc(sizeof(double) * ncsize * (ntri > 0 ? ntri : 1)) : NULL;
     int64_t *nd = (int64_t *)malloc(sizeof(int64_t) * ncsize * (ntri > 0 ? ntri : 1));
@@ -226,7 +262,7 @@ int main(int argc, char **argv)
     float *fn = (float *)malloc(sizeof(float) * ncsize);
     int32_t *in = (int32_t *)malloc(sizeof(int32_t) * ncsize);
     for (int t = 0; t < ntri; ++t) {
-        const int rp = rp_begin + t, r1 = tri[3 * t], r2 = tri[3 * t + 1], r3 = tri[3 * t + 2];
+        const int rp = rps[t], r1 = tri[3 * t], r2 = tri[3 * t + 1], r3 = tri[3 * t + 2];
         const long ng = amber_cuda_ng1(ctx, r1);
         const double gfact = (1. * ng) / (1. * NN), inv = 1.0 / (ng * ng * 1.);
         const double Num = gfact * gfact * rdata[4 * rp + 3];
@@ -259,7 +295,9 @@ int main(int argc, char **argv)
         }
         fclose(fo);
     }
-    printf("AMBER_GPU_JSON {\"triangles\": %d, \"products\": %.17g, \"device_ms\": %.3f}\n", ntri, products, ms);
+    printf("AMBER_GPU_JSON {\"triangles\": %d, \"products\": %.17g, \"device_ms\": %.3f, \"rank\": %d, "
+           "\"world\": %d}\n",
+           ntri, products, ms, rank, world);
     amber_cuda_destroy(ctx);
     return 0;
 }

@@ -525,6 +525,9 @@ def main():
                     help="time the gridding stage alone (100k records x 128 channels onto 256^2)")
     ap.add_argument("--config4", action="store_true",
                     help="measure a fixed sample of the large cube (512^2, 384 channels) instead of the headline")
+    ap.add_argument("--shard", action="store_true",
+                    help="strong scaling: the single-realisation case's triangles split across the ranks "
+                         "(amber_cuda_shard_plan), instead of the headline")
     ap.add_argument("--profile-triangle", type=int, default=-1, metavar="RP",
                     help="profiling runs: triangle RP of the single-realisation case, twice, v1, on --precision")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
@@ -587,6 +590,46 @@ def main():
         t = torch.tensor([x], dtype=torch.float64, device=dev)
         dist.all_reduce(t, op=op)
         return float(t.item())
+
+    if args.shard:
+        from amber_b200 import shard
+        real = synth.config2(seed=1)
+        stream = torch.cuda.current_stream(dev)
+        with amber_b200.Estimator(device=local, precision="mixed", stream=stream.cuda_stream) as est:
+            est.load_grid(real.gv, real.counts, real.du, real.flag_key)
+            est.set_rings(real.ulow, real.uhigh)
+            est.set_channels(real.nc10, real.uf_chans)
+            tri = est.calcr()[:, :3].astype(np.int32)
+            mine = shard.plan_native(tri, est.ng1, world)[rank]
+            sub = tri[mine]
+            for _ in range(args.warmup):
+                est.run(sub, want_v2=True)
+            clocks = Clocks(local)
+            clocks.start()
+            barrier()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            prod = 0.0
+            for _ in range(args.steps):
+                est.run(sub, want_v2=True)
+                prod += est.last_run_stats()[0]
+            e1.record(stream)
+            barrier()
+            clk = clocks.stop()
+            ms = reduce(e0.elapsed_time(e1), dist.ReduceOp.MAX if world > 1 else None)
+            total = reduce(prod, dist.ReduceOp.SUM if world > 1 else None)
+            planned = {str(n): shard.planned_speedup(tri, est.ng1, n) for n in (1, 2, 4, 8)}
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": total / (ms * 1e-3), "unit": UNIT, "n_gpus": world,
+                              "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+                              "higher_is_better": True, "scaling": "strong", "impl": "amber_b200",
+                              "dtype": "int8 tensor-core digits, int32 accumulate, fp64 reduce", "data": "synthetic",
+                              "config": {"workload": SINGLE, "parallelism": f"triangles sharded x{world}"},
+                              "triangles_per_rank_0": len(mine), "planned_speedup": planned, "clocks": clk}))
+        if world > 1:
+            dist.barrier()
+            dist.destroy_process_group()
+        return 0
 
     # ---- this rank's ensemble, its cubes resident in HBM ----
     t_gen = time.perf_counter()

@@ -103,6 +103,17 @@ AMBER_API int amber_cuda_calcr(amber_cuda_ctx *ctx, int max_tri, int *rcount, do
 /* Padded map side of a triangle whose largest ring is r1 (amber.c:193-197). */
 AMBER_API long amber_cuda_ng1(const amber_cuda_ctx *ctx, int r1);
 
+/* Strong scaling of one realisation over `world` processes (one per GPU): which rank computes
+ * each of `ntri` closed triangles, given each triangle's largest ring r1 and that ring's map
+ * side ng1 (amber_cuda_ng1).  A triangle is computed whole on one rank, so every lag array is
+ * the single-process one; an r1 group (triangles sharing their maps) whose cost, ng1² per
+ * triangle, is above 1/world of the total is split into ceil(cost·world/total) near-equal
+ * parts, every other group stays whole, and the parts go largest first to the least-loaded
+ * rank, each charged a twenty-fifth of its group's cost for the maps it builds.  Host-only (no
+ * GPU, no context), integer arithmetic: every rank computes the same plan.  rank_of[ntri] out.
+ * No reference counterpart (the reference runs one process per realisation). */
+AMBER_API int amber_cuda_shard_plan(int ntri, const int *r1, const long *ng1, int world, int *rank_of);
+
 /* ---- one triangle, file-ready: replaces the body of the rp loop,
  * amber.c:189-304 (v1) and amber_v2.c:189-309 (v2): fill_s2d_float ×3
  * (+ fill_s2I ×3), the OpenMP triple-product loop and the writer's scalars.

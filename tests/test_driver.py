@@ -70,6 +70,36 @@ def test_driver_v2_files(tmp_path):
         assert np.abs(nt - z["numtri_v2"][i]).max() <= 1e-6 * np.abs(z["numtri_v2"][i]).max()
 
 
+@pytest.mark.parametrize("version", [1, 2])
+def test_driver_sharded_ranks_write_the_single_process_files(tmp_path, version):
+    """Under RANK / WORLD_SIZE each process writes only its share of the triangles (the library's
+    shard plan), and the union of the ranks' files is byte for byte the single-process output.
+    The two ranks run one after the other on the same GPU (nothing waits on the other)."""
+    from amber_b200 import build
+    build.build()
+    z = np.load(os.path.join(GOLDEN, "est_flagged48.npz"))
+    real = _real_from(z)
+    single, _ = _run(real, tmp_path, version, "mixed")
+    exe = os.path.join(os.path.dirname(build.LIB), "amber_gpu")
+    shared = tmp_path / "sharded"
+    counts = []
+    for rank in range(2):
+        env = dict(os.environ, RANK=str(rank), WORLD_SIZE="2", LOCAL_RANK="0")
+        p = subprocess.run([exe, "1", f"v{version}", str(real.nc10), str(tmp_path / "rings.txt"), "0", "-1",
+                            str(shared), str(tmp_path / "input_params_ess"), "mixed"],
+                           capture_output=True, text=True, cwd=tmp_path, env=env)
+        assert p.returncode == 0, p.stderr
+        st = json.loads([ln for ln in p.stdout.splitlines() if ln.startswith("AMBER_GPU_JSON ")][-1][15:])
+        assert (st["rank"], st["world"]) == (rank, 2)
+        counts.append(st["triangles"])
+    assert sum(counts) == len(z["rdata"]) and min(counts) > 0
+    names = sorted(os.listdir(single))
+    assert names == sorted(os.listdir(shared))
+    for n in names:
+        with open(os.path.join(single, n), "rb") as a, open(os.path.join(shared, n), "rb") as b:
+            assert a.read() == b.read(), n
+
+
 def _run_vcg(tmp, z, collapse, fwhm=1480.73):
     from amber_b200 import build
     build.build()
