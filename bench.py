@@ -29,7 +29,9 @@ per triangle total_vcp·Ng1², counted for the D and the I (mask) sums.
 * cpu_baseline — the reference's own OpenMP loop (oracle/_ref/ref_amber_fast,
   its sources built unchanged) on the host cores, one triangle of the ensemble;
 * single_realisation — the 256², 128-channel, 16-bin realisation on the
-  device-resident path.
+  device-resident path;
+* config4_sample — six triangles of the 512², 384-channel cube (all four with
+  Ng1 = 1460), with the plain FP64 path and its error on one more.
 
 `--impl reference` times that same reference build as the reference arm.
 `--serving N`, `--config4`, `--config1`, `--stages`, `--maps`, `--gridding` run
@@ -268,7 +270,7 @@ def serving_section(amber_b200, synth, dev, n=200, rate=0.2):
     scale = 50.0 / rate
     with amber_b200.Estimator(device=dev, precision="mixed") as est:
         eng = amber_b200.Engine(est)
-        run_batch(eng, [synth.from_spec(dict(reqs[0], nn=64, nc=32))], [0])  # warm-up
+        run_batch(eng, [synth.from_spec(dict(reqs[0], nn=64, nc=32, nc10=15, ring_hi=30.0))], [0])  # warm-up
         s0 = eng.stats()
         t0 = time.perf_counter()
         tickets = []
@@ -512,6 +514,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-single", action="store_true", help="skip the single-realisation section")
+    ap.add_argument("--no-config4", action="store_true", help="skip the large-cube sample section")
     ap.add_argument("--serving", type=int, default=0, metavar="N",
                     help="run N requests of the serving stream instead of the headline")
     ap.add_argument("--rate", type=float, default=0.2, help="Poisson arrival rate of --serving (req/s)")
@@ -745,6 +748,11 @@ def main():
             out["single_realisation"] = single_section(amber_b200, synth, local, stream)
         except Exception as ex:
             out["single_realisation"] = {"error": str(ex)[:300]}
+    if rank == 0 and world == 1 and not args.no_config4:
+        try:
+            out["config4_sample"] = config4_section(amber_b200, synth, local, args)
+        except Exception as ex:
+            out["config4_sample"] = {"error": str(ex)[:300]}
     if rank == 0 and not args.no_cpu_baseline:
         try:
             import oracle
