@@ -47,11 +47,19 @@ __device__ __forceinline__ bool in_ring(long ia, long j, double lo, double hi)
     return uu >= lo && uu < hi && uu > 0.0;
 }
 
+// Ring edges and column counts of the slots one launch builds, passed by value: no upload and no
+// stream synchronisation before the launch, so the host can queue the next request's maps while
+// these run.  A batch with more slots runs as several launches.
+constexpr int RING_META_MAX = 96;
+struct RingMeta {
+    double lo[RING_META_MAX], hi[RING_META_MAX];
+    int jc[RING_META_MAX];
+};
+
 template <int C>
 __global__ void __launch_bounds__(kThreads) ring_cols_kernel(const void *__restrict__ src, int src_complex, long n1,
                                                               long nc, long chan_base, long nch, long ng,
-                                                              const double *__restrict__ lohi,
-                                                              const int *__restrict__ jcols, int jmax,
+                                                              const RingMeta meta, int jmax,
                                                               const double2 *__restrict__ tw_g,
                                                               double2 *__restrict__ Y, int rowcap)
 {
@@ -64,8 +72,8 @@ __global__ void __launch_bounds__(kThreads) ring_cols_kernel(const void *__restr
 
     const int j = blockIdx.x, s = blockIdx.y;
     const long q0 = (long)blockIdx.z * C;
-    if (j >= jcols[s]) return;
-    const double lo = lohi[2 * s], hi = lohi[2 * s + 1];
+    if (j >= meta.jc[s]) return;
+    const double lo = meta.lo[s], hi = meta.hi[s];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const long h1 = n1 / 2 + 1;
 
@@ -171,7 +179,7 @@ __device__ __forceinline__ uint16_t bf16_bits(float f)
 
 template <int C>
 __global__ void __launch_bounds__(kThreads) ring_rows_kernel(const double2 *__restrict__ Y, long ng, int jmax,
-                                                              const int *__restrict__ jcols, long nch,
+                                                              const RingMeta meta, long nch,
                                                               const double2 *__restrict__ tw_g, long kp,
                                                               double *__restrict__ out_f64,
                                                               uint16_t *__restrict__ out_hi,
@@ -185,7 +193,7 @@ __global__ void __launch_bounds__(kThreads) ring_rows_kernel(const double2 *__re
     const long n0 = blockIdx.x;
     const int s = blockIdx.y;
     const long q0 = (long)blockIdx.z * C;
-    const int J = jcols[s];
+    const int J = meta.jc[s];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     for (long i = tid; i < ng; i += kThreads) tw[i] = tw_g[i];
     for (int e = tid; e < J * C; e += kThreads) {
@@ -376,23 +384,6 @@ int build_maps(amber_cuda_ctx *c, const MapJob &job)
     const double2 *tw;
     int rc = twiddle_table(c, ng, &tw);
     if (rc) return rc;
-    // device copies of lo/hi and column counts
-    size_t meta = sizeof(double) * 2 * job.nslots + sizeof(int) * job.nslots;
-    if ((rc = ensure(c, c->ring_lohi, meta, "ring metadata"))) return rc;
-    std::vector<unsigned char> hbuf(meta);
-    for (int s = 0; s < job.nslots; ++s) {
-        reinterpret_cast<double *>(hbuf.data())[2 * s] = job.lo[s];
-        reinterpret_cast<double *>(hbuf.data())[2 * s + 1] = job.hi[s];
-    }
-    memcpy(hbuf.data() + sizeof(double) * 2 * job.nslots, jc.data(), sizeof(int) * job.nslots);
-    if ((rc = cuda_check(c, cudaMemcpyAsync(c->ring_lohi.p, hbuf.data(), meta, cudaMemcpyHostToDevice, c->stream),
-                         "upload ring metadata")))
-        return rc;
-    if ((rc = cuda_check(c, cudaStreamSynchronize(c->stream), "ring metadata sync"))) return rc;
-    const double *d_lohi = reinterpret_cast<const double *>(c->ring_lohi.p);
-    const int *d_jc = reinterpret_cast<const int *>(reinterpret_cast<const unsigned char *>(c->ring_lohi.p) +
-                                                    sizeof(double) * 2 * job.nslots);
-
     size_t ybytes = sizeof(double2) * (size_t)job.nslots * ng * jmax * job.nch;
     if ((rc = ensure(c, c->y, ybytes, "map intermediate"))) return rc;
     double2 *Y = reinterpret_cast<double2 *>(c->y.p);
@@ -403,51 +394,64 @@ int build_maps(amber_cuda_ctx *c, const MapJob &job)
     int C1 = 32;
     while (C1 > 1 && p1_smem(C1) > smem_cap) C1 /= 2;
     if (p1_smem(C1) > smem_cap) return fail(c, AMBER_ERR_ARG, "ring too wide for the column stage (%d rows)", rows_max);
-    dim3 g1(jmax, job.nslots, (unsigned)((job.nch + C1 - 1) / C1));
-    size_t s1 = p1_smem(C1);
+    const size_t s1 = p1_smem(C1);
+    auto p2_smem = [&](int C) { return sizeof(double2) * ng + sizeof(double2) * C * jmax; };
+    int C2 = 32;
+    while (C2 > 1 && p2_smem(C2) > smem_cap) C2 /= 2;
+    const size_t s2 = p2_smem(C2);
+    // up to RING_META_MAX slots per launch pair, each launch's pointers offset to its first slot
+    for (int sb = 0; sb < job.nslots; sb += RING_META_MAX) {
+        const int ns = std::min(RING_META_MAX, job.nslots - sb);
+        RingMeta meta;
+        for (int i = 0; i < ns; ++i) {
+            meta.lo[i] = job.lo[sb + i];
+            meta.hi[i] = job.hi[sb + i];
+            meta.jc[i] = jc[sb + i];
+        }
+        double2 *Ys = Y + (size_t)sb * ng * jmax * job.nch;
+        const size_t so = (size_t)sb * job.nch * job.kp;
+        double *of64 = job.out_f64 ? job.out_f64 + so : nullptr;
+        uint16_t *ohi = job.out_hi ? job.out_hi + so : nullptr, *olo = job.out_lo ? job.out_lo + so : nullptr;
+        float *of32 = job.out_f32 ? job.out_f32 + so : nullptr;
+        dim3 g1(jmax, ns, (unsigned)((job.nch + C1 - 1) / C1));
 #define LAUNCH_COLS(CC)                                                                                        \
     do {                                                                                                        \
         cudaFuncSetAttribute(ring_cols_kernel<CC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s1);        \
         ring_cols_kernel<CC><<<g1, kThreads, s1, c->stream>>>(job.src, job.src_complex ? 1 : 0, job.n1, job.nc, \
-                                                               job.chan_base, job.nch, ng, d_lohi, d_jc, jmax,  \
-                                                               tw, Y, rows_max);                                \
+                                                               job.chan_base, job.nch, ng, meta, jmax, tw, Ys,  \
+                                                               rows_max);                                        \
     } while (0)
-    switch (C1) {
-        case 32: LAUNCH_COLS(32); break;
-        case 16: LAUNCH_COLS(16); break;
-        case 8: LAUNCH_COLS(8); break;
-        case 4: LAUNCH_COLS(4); break;
-        case 2: LAUNCH_COLS(2); break;
-        default: LAUNCH_COLS(1); break;
-    }
+        switch (C1) {
+            case 32: LAUNCH_COLS(32); break;
+            case 16: LAUNCH_COLS(16); break;
+            case 8: LAUNCH_COLS(8); break;
+            case 4: LAUNCH_COLS(4); break;
+            case 2: LAUNCH_COLS(2); break;
+            default: LAUNCH_COLS(1); break;
+        }
 #undef LAUNCH_COLS
-    c->launches += 1;
-    if ((rc = cuda_check(c, cudaGetLastError(), "ring_cols_kernel launch"))) return rc;
+        c->launches += 1;
+        if ((rc = cuda_check(c, cudaGetLastError(), "ring_cols_kernel launch"))) return rc;
 
-    // pass 2
-    auto p2_smem = [&](int C) { return sizeof(double2) * ng + sizeof(double2) * C * jmax; };
-    int C2 = 32;
-    while (C2 > 1 && p2_smem(C2) > smem_cap) C2 /= 2;
-    dim3 g2((unsigned)ng, job.nslots, (unsigned)((job.nch + C2 - 1) / C2));
-    size_t s2 = p2_smem(C2);
+        dim3 g2((unsigned)ng, ns, (unsigned)((job.nch + C2 - 1) / C2));
 #define LAUNCH_ROWS(CC)                                                                                        \
     do {                                                                                                        \
         cudaFuncSetAttribute(ring_rows_kernel<CC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s2);        \
-        ring_rows_kernel<CC><<<g2, kThreads, s2, c->stream>>>(Y, ng, jmax, d_jc, job.nch, tw, job.kp,          \
-                                                               job.out_f64, job.out_hi, job.out_lo, job.out_f32,  \
-                                                               job.weight);                                       \
+        ring_rows_kernel<CC><<<g2, kThreads, s2, c->stream>>>(Ys, ng, jmax, meta, job.nch, tw, job.kp, of64, ohi, \
+                                                               olo, of32, job.weight);                           \
     } while (0)
-    switch (C2) {
-        case 32: LAUNCH_ROWS(32); break;
-        case 16: LAUNCH_ROWS(16); break;
-        case 8: LAUNCH_ROWS(8); break;
-        case 4: LAUNCH_ROWS(4); break;
-        case 2: LAUNCH_ROWS(2); break;
-        default: LAUNCH_ROWS(1); break;
-    }
+        switch (C2) {
+            case 32: LAUNCH_ROWS(32); break;
+            case 16: LAUNCH_ROWS(16); break;
+            case 8: LAUNCH_ROWS(8); break;
+            case 4: LAUNCH_ROWS(4); break;
+            case 2: LAUNCH_ROWS(2); break;
+            default: LAUNCH_ROWS(1); break;
+        }
 #undef LAUNCH_ROWS
-    c->launches += 1;
-    if ((rc = cuda_check(c, cudaGetLastError(), "ring_rows_kernel launch"))) return rc;
+        c->launches += 1;
+        if ((rc = cuda_check(c, cudaGetLastError(), "ring_rows_kernel launch"))) return rc;
+    }
     if (job.dig) {
         const long nblk = job.kp / LS_BLOCK;
         dim3 gq((unsigned)nblk, (unsigned)job.nslots);
