@@ -753,7 +753,7 @@ def main():
             out["config4_sample"] = config4_section(amber_b200, synth, local, args)
         except Exception as ex:
             out["config4_sample"] = {"error": str(ex)[:300]}
-    if rank == 0 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             import oracle
             if oracle.ref_available():
