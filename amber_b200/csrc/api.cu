@@ -322,7 +322,7 @@ int run_next_batch(amber_cuda_ctx *c, RunState &st, std::vector<I8Job> *jobs)
         ms.ring_of_slot.push_back(r);
     }
     ms.nslots = (int)ms.ring_of_slot.size();
-    const size_t nvals = (size_t)ms.nslots * c->nc * kp, nrows = (size_t)ms.nslots * c->nc;
+    const size_t nvals = (size_t)ms.nslots * c->nc * kp;
     if ((rc = ensure(c, c->maps_d, per_slot * ms.nslots, "ring maps"))) return rc;
     if (want_v2 && (rc = ensure(c, c->maps_i, per_slot * ms.nslots, "ring mask maps"))) return rc;
     // carve one map set (D or I) out of its buffer
