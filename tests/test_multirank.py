@@ -118,5 +118,20 @@ def test_library_plan_equals_the_python_plan():
             assert shard.plan_native(tri, ng, world) == shard.plan(tri, ng, world), world
 
 
+def test_library_plan_rejects_bad_arguments():
+    import ctypes
+    from amber_b200 import load_library
+    L = load_library()
+    r1 = (ctypes.c_int * 2)(0, 1)
+    ng = (ctypes.c_long * 2)(10, 12)
+    out = (ctypes.c_int * 2)()
+    assert L.amber_cuda_shard_plan(2, r1, ng, 0, out) == -1       # no ranks
+    bad = (ctypes.c_long * 2)(10, 0)
+    assert L.amber_cuda_shard_plan(2, r1, bad, 2, out) == -1      # a map side of 0
+    assert L.amber_cuda_shard_plan(2, r1, ng, 3, out) == 0        # more ranks than triangles: fine
+    assert sorted(out) == [0, 1]
+    assert L.amber_cuda_shard_plan(0, None, None, 4, None) == 0   # nothing to plan
+
+
 def test_rank_seeds_differ():
     assert len({shard.rank_seed(1, r) for r in range(8)}) == 8
