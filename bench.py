@@ -257,7 +257,7 @@ def fp64_section(amber_b200, torch, reals, cubes, dev, mixed_sub):
             "err_sample": sorted(mixed_sub)}
 
 
-def serving_section(amber_b200, synth, dev, n=200, rate=0.2):
+def serving_section(amber_b200, synth, dev, n=200, rate=0.3):
     """Serving stream: ``n`` requests of the config-5 size distribution (sides {64,128,256,384},
     16-256 channels, 6-20 bins, own seed and flags) arriving as a Poisson process at ``rate``
     req/s (the stream's 50 req/s inter-arrival times rescaled), enqueued at their arrival times;
@@ -517,7 +517,8 @@ def main():
     ap.add_argument("--no-config4", action="store_true", help="skip the large-cube sample section")
     ap.add_argument("--serving", type=int, default=0, metavar="N",
                     help="run N requests of the serving stream instead of the headline")
-    ap.add_argument("--rate", type=float, default=0.2, help="Poisson arrival rate of --serving (req/s)")
+    ap.add_argument("--rate", type=float, default=0.3,
+                    help="Poisson arrival rate of --serving (req/s); one B200 serves ~0.41/s of the stream's sizes")
     ap.add_argument("--config1", action="store_true",
                     help="measure the reference's whole CPU-runnable case (config 1) beside the reference's own run")
     ap.add_argument("--stages", action="store_true",
