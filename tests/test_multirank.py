@@ -118,6 +118,34 @@ def test_library_plan_equals_the_python_plan():
             assert shard.plan_native(tri, ng, world) == shard.plan(tri, ng, world), world
 
 
+def test_library_plan_equals_the_python_plan_on_random_lists():
+    """Seeded random triangle lists: uneven r1 groups, map sides with ties and large spreads,
+    unsorted input and 1-16 ranks.  The C and Python plans agree triangle for triangle, each covers
+    every triangle once, and a group within 1/N of the cost stays on one rank."""
+    rng = np.random.default_rng(20261204)
+    for case in range(150):
+        nr = int(rng.integers(1, 25))
+        ntri = int(rng.integers(1, 400))
+        side = np.sort(rng.integers(8, 1500, size=nr))
+        if case % 3 == 0:
+            side[:] = side[0]  # every group the same map side: ties throughout the ordering
+        r1 = rng.integers(0, nr, size=ntri)
+        tri = np.stack([r1, r1, r1], axis=1)
+        ng = lambda r, side=side: int(side[r])
+        world = int(rng.integers(1, 17))
+        want = shard.plan(tri, ng, world)
+        assert shard.plan_native(tri, ng, world) == want, (case, world)
+        assert sorted(i for p in want for i in p) == list(range(ntri))
+        cost = {}
+        for r in r1.tolist():
+            cost[r] = cost.get(r, 0) + ng(r) ** 2
+        total = sum(cost.values())
+        for r, c in cost.items():
+            if c * world <= total:
+                holders = [k for k, p in enumerate(want) if any(r1[i] == r for i in p)]
+                assert len(holders) == 1, (case, r, holders)
+
+
 def test_library_plan_rejects_bad_arguments():
     import ctypes
     from amber_b200 import load_library
