@@ -161,5 +161,31 @@ def test_library_plan_rejects_bad_arguments():
     assert L.amber_cuda_shard_plan(0, None, None, 4, None) == 0   # nothing to plan
 
 
+def test_ranks_get_the_same_ensemble_shapes_with_their_own_seeds():
+    """Weak scaling: every rank's 64-realisation ensemble has the same grid sides, channel counts,
+    bins and lag windows; only the data seeds (and so the fields, sampling and flags) differ."""
+    base = synth.config3_specs()
+    for rank in (1, 7):
+        other = synth.config3_specs(seed0=100 + 64 * rank)
+        shape = lambda sp: (sp["nn"], sp["nc"], sp["nbins"], sp["ring_lo"], sp["ring_hi"], sp["nc10"], sp["flag_frac"])
+        assert [shape(a) for a in base] == [shape(b) for b in other]
+        assert not {a["seed"] for a in base} & {b["seed"] for b in other}
+
+
+def test_sharded_gather_rejects_duplicates_and_gaps():
+    """estimate_sharded on rank 0 refuses a gather in which a triangle arrives twice or not at all
+    (host logic, no process group: the gather is a plain function)."""
+    tri = np.array([[2, 1, 1], [2, 2, 1], [3, 1, 1], [3, 3, 2]])
+    ng = lambda r1: 40 + 10 * r1
+    compute = lambda idx: {i: i * 10 for i in idx}
+    assert shard.estimate_sharded(tri, ng, compute, 0, 2, lambda obj: [compute(p) for p in shard.plan(tri, ng, 2)]) \
+        == [0, 10, 20, 30]
+    assert shard.estimate_sharded(tri, ng, compute, 1, 2, lambda obj: [obj, obj]) is None  # other ranks: nothing
+    with pytest.raises(RuntimeError, match="computed twice"):
+        shard.estimate_sharded(tri, ng, compute, 0, 2, lambda obj: [compute([0, 1, 2, 3]), compute([0])])
+    with pytest.raises(RuntimeError, match="gathered 3 of 4"):
+        shard.estimate_sharded(tri, ng, compute, 0, 2, lambda obj: [compute([0, 1]), compute([2])])
+
+
 def test_rank_seeds_differ():
     assert len({shard.rank_seed(1, r) for r in range(8)}) == 8
