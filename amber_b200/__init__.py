@@ -159,6 +159,7 @@ def load_library():
     L.amber_cuda_result.argtypes = [_vp, ctypes.c_int64, ctypes.c_int, _dp, _dp, _i64p, _dp, _dp, _dp]
     L.amber_cuda_engine_stats.argtypes = [_vp, ctypes.POINTER(EngineInfo)]
     L.amber_cuda_tile_choices.argtypes = [_vp, ctypes.c_int, _ip, _ip, _fp, _fp]
+    L.amber_cuda_shard_plan.argtypes = [ctypes.c_int, _ip, ctypes.POINTER(ctypes.c_long), ctypes.c_int, _ip]
     L.amber_cuda_grid_vis_collapsed.argtypes = [_vp, ctypes.c_long, ctypes.c_long, ctypes.c_double, ctypes.c_double,
                                                 ctypes.c_float, ctypes.c_int, ctypes.c_long, ctypes.c_long,
                                                 ctypes.c_long, _fp, _fp, ctypes.c_long, _dp, _dp]
