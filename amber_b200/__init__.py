@@ -133,6 +133,7 @@ def load_library():
     L.amber_cuda_last_error.restype = ctypes.c_char_p
     L.amber_cuda_load_grid_packed.argtypes = [_vp, ctypes.c_long, ctypes.c_long, ctypes.c_double, ctypes.c_int, _dp,
                                               _dp]
+    L.amber_cuda_load_grid_device.argtypes = L.amber_cuda_load_grid_packed.argtypes
     L.amber_cuda_load_grid.argtypes = [_vp, ctypes.c_long, ctypes.c_long, ctypes.c_double, ctypes.c_int,
                                        ctypes.POINTER(_dp), ctypes.POINTER(_dp), ctypes.POINTER(_dp)]
     L.amber_cuda_set_rings.argtypes = [_vp, ctypes.c_int, _dp, _dp]
