@@ -21,6 +21,13 @@ outputs as compressed .npz files:
 
 Needs the reference sources (make -C oracle ref); run from the repo root:
     python tests/golden/make_golden.py
+
+Reproducibility: the reference's accumulation loop is an OpenMP loop whose
+partial sums are added in thread-schedule order, so a fresh run reproduces the
+lag arrays to rounding only (within 3e-16 of the largest value for the FP64
+build, 1e-7 for the float build); the triangle lists, counts, gridding, MAPS and
+cylindrical-bispectrum outputs come out bit-identical.  The tests compare with
+tolerances far above that (1e-10 of the per-cell sum of |products| for FP64).
 """
 from __future__ import annotations
 
