@@ -114,6 +114,12 @@ int main(int argc, char **argv)
         fprintf(stderr, "GV_data: short header\n");
         exit(EXIT_FAILURE);
     }
+    /* the gridding stage writes an even NN = 2·ceil(Umax/dU) and Du > 0; the bounds keep the
+     * buffer sizes below from wrapping on a file that is not a grid */
+    if (NN <= 0 || NN % 2 || NN > (1 << 20) || nc <= 0 || nc > (1 << 20) || !(Du > 0)) {
+        fprintf(stderr, "GV_data: bad header (NN %lld, nc %lld, Du %g)\n", (long long)NN, (long long)nc, Du);
+        exit(EXIT_FAILURE);
+    }
     const size_t ncell = (size_t)NN * (NN / 2 + 1);
     double *re_im = (double *)malloc(sizeof(double) * 2 * ncell * nc);
     double *ntig = (double *)malloc(sizeof(double) * ncell * nc);
@@ -167,8 +173,13 @@ int main(int argc, char **argv)
         if (!fp) die("Error opening file");
         int cap = 64, v;
         uf = (int *)malloc(sizeof(int) * cap);
+        if (!uf) die("malloc");
         while (fscanf(fp, "%d", &v) == 1) {
-            if (uf_nc == cap) uf = (int *)realloc(uf, sizeof(int) * (cap *= 2));
+            if (uf_nc == cap) {
+                int *grown = (int *)realloc(uf, sizeof(int) * (cap *= 2));
+                if (!grown) die("realloc");
+                uf = grown;
+            }
             uf[uf_nc++] = v;
         }
         fclose(fp);

@@ -74,7 +74,8 @@ int main(int argc, char *argv[])
     double Du = 0;
     int32_t flag_key = 0;
     if (fread(&NN, 8, 1, fp) != 1 || fread(&nc, 8, 1, fp) != 1 || fread(&Du, 8, 1, fp) != 1 ||
-        fread(&flag_key, 4, 1, fp) != 1 || NN <= 0 || NN % 2 || nc <= 0) {
+        fread(&flag_key, 4, 1, fp) != 1 || NN <= 0 || NN % 2 || NN > (1 << 20) || nc <= 0 || nc > (1 << 20) ||
+        !(Du > 0)) {
         fprintf(stderr, "GV_data: bad header\n");
         return 1;
     }

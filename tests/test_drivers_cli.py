@@ -75,6 +75,30 @@ def test_maps_usage_and_missing_inputs(exes, tmp_path):
     assert p.returncode != 0 and "GV_data" in p.stderr
 
 
+def _bad_grid(path, nn, nc, du):
+    """A GV_data file whose 28-byte header (formats.GV_HEADER) holds the given values, then a little
+    data: the drivers must refuse it before sizing any buffer from it."""
+    with open(path, "wb") as f:
+        f.write(formats.GV_HEADER.pack(nn, nc, du, 0))
+        f.write(bytes(256))
+
+
+@pytest.mark.parametrize("nn,nc,du", [(-4, 3, 0.5), (15, 3, 0.5), (16, 0, 0.5), (16, 3, 0.0),
+                                      (1 << 40, 1 << 40, 0.5)])
+def test_drivers_refuse_a_grid_header_that_is_not_a_grid(exes, tmp_path, nn, nc, du):
+    """A negative, odd or absurd side, no channels or a non-positive cell size: both executables
+    stop with "bad header" and a failure status (the sizes would otherwise wrap malloc and fread)."""
+    data = tmp_path / "data"
+    data.mkdir()
+    _bad_grid(data / "GV_data_1", nn, nc, du)
+    formats.write_input_params_ess(tmp_path / "input_params_ess", 154.255, 0.04, 1.0, str(data))
+    p = _run([exes.DRIVER, "1"], tmp_path)
+    assert p.returncode != 0 and "bad header" in p.stderr, p.stderr
+    (tmp_path / "input_params").write_text(f"32\t0.5\t154.255e6\t40e3\t1\t8\t{data}\n")
+    p = _run([exes.MAPS_DRIVER, "1", "GV_data_1"], tmp_path)
+    assert p.returncode != 0 and "bad header" in p.stderr, p.stderr
+
+
 def test_cylbs_parameter_checks():
     with pytest.raises(ValueError):
         amber_b200.cylbs_params(denominator="both")
