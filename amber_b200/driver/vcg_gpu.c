@@ -73,8 +73,11 @@ static int open_synthetic(const char *path, vis_reader *r)
     char magic[8];
     int64_t h[4];
     float f[4];
+    /* records, random parameters, Stokes and channels; the upper bounds keep every buffer size
+     * below 2^56 bytes, so nothing computed from them wraps */
     if (fread(magic, 1, 8, fp) != 8 || memcmp(magic, "AMBRVIS1", 8) != 0 || fread(h, 8, 4, fp) != 4 ||
-        fread(f, 4, 4, fp) != 4 || h[0] < 0 || h[1] < 2 || h[2] < 1 || h[3] < 1) {
+        fread(f, 4, 4, fp) != 4 || h[0] < 0 || h[0] > ((int64_t)1 << 32) || h[1] < 2 || h[1] > 64 || h[2] < 1 ||
+        h[2] > 16 || h[3] < 1 || h[3] > (1 << 16)) {
         fclose(fp);
         return -2;
     }

@@ -33,6 +33,19 @@ def test_vcg_rejects_a_file_that_is_not_visibilities(exes, tmp_path):
     assert p.returncode == 1 and "not a visibility file" in p.stderr
 
 
+@pytest.mark.parametrize("g,pcount,nstokes,nchan", [(-1, 5, 2, 8), (1 << 40, 5, 2, 8), (10, 1 << 30, 2, 8),
+                                                     (10, 5, 1 << 20, 8), (10, 5, 2, 1 << 40)])
+def test_vcg_rejects_a_visibility_header_out_of_range(exes, tmp_path, g, pcount, nstokes, nchan):
+    """Record, parameter, Stokes and channel counts past what any file holds are refused as "not a
+    visibility file" before any buffer is sized from them."""
+    (tmp_path / "params").write_text("4\t20.0\t1480.73\t1.\n")
+    with open(tmp_path / "vis", "wb") as f:
+        f.write(formats.VIS_HEADER.pack(formats.VIS_MAGIC, g, pcount, nstokes, nchan, 1.5e8, 4e4, 1.0, 0.0))
+        f.write(bytes(64))
+    p = _run([exes.VCG_DRIVER, "vis", "params", "GV", "1", "0", "1", "samp"], tmp_path)
+    assert p.returncode == 1 and "not a visibility file" in p.stderr, p.stderr
+
+
 def test_vcg_rejects_more_channels_than_the_file_holds(exes, tmp_path):
     randpar, data = synth.make_visibilities(16, 1.0254384902642049, 3, 20, 5, umax=8.0)
     formats.write_vis(tmp_path / "vis", randpar, data, np.float32(synth.NU0), 40.0e3, 1.0)
