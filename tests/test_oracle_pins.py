@@ -193,3 +193,25 @@ def test_oracle_matches_reference_at_edges(nn, nc, seed, nc10, flagged):
         assert (np.abs(bl - r["bldnu"]) <= 1e-10 * r["absscale"] + 1e-300).all()
         np.testing.assert_allclose(num, (r["ng1"] / real.nn) ** 2 * r["rdata_num"], rtol=1e-12)
         np.testing.assert_allclose(ntri, num / r["ng1"] ** 2, rtol=1e-12)
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="reference build (oracle/_ref) not present")
+@pytest.mark.parametrize("nn,nc,seed,nc10,flagged", [
+    (32, 6, 26, 0, None),                        # only the zero lag
+    (32, 7, 27, 6, None),                        # nc10 = nc - 1: the widest window
+    (36, 12, 28, 5, [0, 1, 2, 4, 6, 7, 9, 11]),  # most channels flagged
+])
+def test_oracle_v2_matches_reference_at_edges(nn, nc, seed, nc10, flagged):
+    """The same edges for the v2 files (4_fbe/amber_v2.c:295-309): lag sums and sampling-mask sums
+    per lag cell within 1e-10 of their own Σ|products|, and the 1/Ng1² scalar."""
+    real = synth.tiny(nn, nc, seed=seed, nbins=3, hi=0.44 * nn, nc10=nc10, flagged=flagged)
+    st, rp = oracle.run_ref_amber(real, oracle.tmpdir(), version=2, fp64=True)
+    rdata, res = oracle.estimate(real, version=2, with_absscale=True)
+    np.testing.assert_array_equal(formats.read_closed_rings(rp)[:, :3], rdata[:, :3])
+    assert len(res) > 0
+    for r in res:
+        inv, bl, nd = formats.read_bsout_v2(os.path.join(rp, formats.bsout_name(2, r["r1"], r["r2"], r["r3"], 1)),
+                                            real.nclen, np.float64)
+        assert (np.abs(bl - r["bldnu"]) <= 1e-10 * r["absscale"] + 1e-300).all()
+        assert (np.abs(nd - r["numtri"]) <= 1e-10 * r["absscale_i"] + 1e-300).all()
+        assert inv == 1.0 / (r["ng1"] ** 2)
