@@ -215,3 +215,31 @@ def test_oracle_v2_matches_reference_at_edges(nn, nc, seed, nc10, flagged):
         assert (np.abs(bl - r["bldnu"]) <= 1e-10 * r["absscale"] + 1e-300).all()
         assert (np.abs(nd - r["numtri"]) <= 1e-10 * r["absscale_i"] + 1e-300).all()
         assert inv == 1.0 / (r["ng1"] ** 2)
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="reference build (oracle/_ref) not present")
+@pytest.mark.parametrize("version", [1, 2])
+def test_oracle_matches_reference_on_an_empty_realisation(version):
+    """No sampled cell at all (every count and every visibility zero): the reference still lists
+    the geometrically closed triangles, with Num = 0, zero lag and mask sums and the full triplet
+    counts; the oracle gives the same files' contents."""
+    real = synth.tiny(32, 6, seed=29, nbins=3, hi=14.0, nc10=2)
+    real.counts[:] = 0.0
+    real.gv[:] = 0.0
+    st, rp = oracle.run_ref_amber(real, oracle.tmpdir(), version=version, fp64=True)
+    rdata, res = oracle.estimate(real, version=version)
+    ref_rings = formats.read_closed_rings(rp)
+    np.testing.assert_array_equal(ref_rings, rdata)
+    assert len(res) == len(ref_rings) > 0 and (ref_rings[:, 3] == 0).all()
+    for r in res:
+        name = os.path.join(rp, formats.bsout_name(version, r["r1"], r["r2"], r["r3"], 1))
+        if version == 1:
+            ntri, num, bl, nd = formats.read_bsout_v1(name, real.nclen, bl_dtype=np.float64)
+            assert ntri == 0.0 and num == 0.0
+            np.testing.assert_array_equal(nd, r["numdnu"])
+            assert nd.max() > 0
+        else:
+            inv, bl, nd = formats.read_bsout_v2(name, real.nclen, np.float64)
+            assert inv == 1.0 / (r["ng1"] ** 2)
+            assert not nd.any() and not r["numtri"].any()
+        assert not bl.any() and not r["bldnu"].any()
