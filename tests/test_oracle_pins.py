@@ -243,3 +243,26 @@ def test_oracle_matches_reference_on_an_empty_realisation(version):
             assert inv == 1.0 / (r["ng1"] ** 2)
             assert not nd.any() and not r["numtri"].any()
         assert not bl.any() and not r["bldnu"].any()
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="reference build (oracle/_ref) not present")
+@pytest.mark.parametrize("version", [1, 2])
+def test_oracle_matches_reference_with_whole_cell_ring_edges(version):
+    """Ring edges at whole cells, as the reference's own annular_rings ladder has them
+    (4_fbe/amber_funcs.c:2022-2062): cells whose radius falls exactly on an edge belong to the outer
+    ring (lo ≤ √(ia²+j²) < hi).  Triangle list, Num and counts exact, sums within 1e-10."""
+    import dataclasses
+    real = synth.tiny(40, 8, seed=31, nbins=4, hi=17.0, nc10=3, flagged=[2])
+    real = dataclasses.replace(real, ulow=np.array([1.0, 5.0, 10.0, 15.0]), uhigh=np.array([5.0, 10.0, 15.0, 17.0]))
+    st, rp = oracle.run_ref_amber(real, oracle.tmpdir(), version=version, fp64=True)
+    rdata, res = oracle.estimate(real, version=version, with_absscale=True)
+    np.testing.assert_array_equal(formats.read_closed_rings(rp), rdata)
+    for r in res:
+        name = os.path.join(rp, formats.bsout_name(version, r["r1"], r["r2"], r["r3"], 1))
+        if version == 1:
+            ntri, num, bl, nd = formats.read_bsout_v1(name, real.nclen, bl_dtype=np.float64)
+            np.testing.assert_array_equal(nd, r["numdnu"])
+        else:
+            inv, bl, nd = formats.read_bsout_v2(name, real.nclen, np.float64)
+            assert (np.abs(nd - r["numtri"]) <= 1e-10 * r["absscale_i"] + 1e-300).all()
+        assert (np.abs(bl - r["bldnu"]) <= 1e-10 * r["absscale"] + 1e-300).all()
