@@ -266,3 +266,27 @@ def test_oracle_matches_reference_with_whole_cell_ring_edges(version):
             inv, bl, nd = formats.read_bsout_v2(name, real.nclen, np.float64)
             assert (np.abs(nd - r["numtri"]) <= 1e-10 * r["absscale_i"] + 1e-300).all()
         assert (np.abs(bl - r["bldnu"]) <= 1e-10 * r["absscale"] + 1e-300).all()
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="reference build (oracle/_ref) not present")
+@pytest.mark.parametrize("version", [1, 2])
+def test_oracle_matches_reference_at_the_archived_cell_size(version):
+    """Du = 1.0254384902642049, the cell size of the reference's archived run (input_params_ess:7):
+    map sides from the Ng1 formula at a non-dyadic Du (amber.c:193-197), the v1 Num scaling and the
+    v2 1/Ng1² scalar, counts exact and sums within 1e-10 of Σ|products|."""
+    real = synth.make_realisation(36, 8, 33, 4, 2.0, 15.0, 3, flagged=[1, 6], du=1.0254384902642049)
+    st, rp = oracle.run_ref_amber(real, oracle.tmpdir(), version=version, fp64=True)
+    rdata, res = oracle.estimate(real, version=version, with_absscale=True)
+    np.testing.assert_array_equal(formats.read_closed_rings(rp), rdata)
+    assert len({r["ng1"] for r in res}) > 1
+    for r in res:
+        name = os.path.join(rp, formats.bsout_name(version, r["r1"], r["r2"], r["r3"], 1))
+        if version == 1:
+            ntri, num, bl, nd = formats.read_bsout_v1(name, real.nclen, bl_dtype=np.float64)
+            np.testing.assert_array_equal(nd, r["numdnu"])
+            np.testing.assert_allclose(num, (r["ng1"] / real.nn) ** 2 * r["rdata_num"], rtol=1e-12)
+        else:
+            inv, bl, nd = formats.read_bsout_v2(name, real.nclen, np.float64)
+            assert inv == 1.0 / (r["ng1"] ** 2)
+            assert (np.abs(nd - r["numtri"]) <= 1e-10 * r["absscale_i"] + 1e-300).all()
+        assert (np.abs(bl - r["bldnu"]) <= 1e-10 * r["absscale"] + 1e-300).all()
