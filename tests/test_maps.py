@@ -50,6 +50,18 @@ def test_oracle_matches_fresh_reference_run():
     assert len(lines) == 10 * 7 and lines[0].split("\t")[0] == "0"
 
 
+@pytest.mark.skipif(not oracle.ref_available(), reason="reference build (oracle/_ref) not present")
+def test_oracle_matches_fresh_reference_run_with_the_last_channel_flagged():
+    """Flagged channels, the last among them: the reference prints the last pair's bin means, so
+    binu and num come out zero, and every value still equals the reference's bit for bit."""
+    real = synth.tiny(32, 7, seed=57, nbins=3, hi=14.0, flagged=[2, 6])
+    r, _ = oracle.run_ref_maps(real, oracle.tmpdir(), 10, 0.8, 20.0)
+    o = oracle.cl_dnu(real, 10, 0.8, 20.0)
+    for k in KEYS:
+        np.testing.assert_array_equal(o[k], r[k], err_msg=k)
+    assert not np.any(r["binu"]) and not np.any(r["num"]) and np.any(r["cldnu"])
+
+
 def _device(real, nb, umin, umax):
     import amber_b200
     with amber_b200.Estimator(precision="fp64") as est:
