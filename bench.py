@@ -49,7 +49,6 @@ import shutil
 import subprocess
 import sys
 import tempfile
-import threading
 import time
 
 import numpy as np
@@ -132,7 +131,6 @@ class Clocks:
 def cpu_reference_sample(real, nthreads=None, rp_pick=None, version=1, fast=True):
     """Time the reference's own accumulation loop (ref_amber_fast) on one triangle."""
     import oracle  # the reference build and its driver live in oracle/
-    from amber_b200 import formats
     wd = tempfile.mkdtemp(prefix="amber_ref_")
     try:
         nthreads = nthreads or os.cpu_count() or 1

@@ -38,7 +38,7 @@ def lib_built():
 
 
 def _run(real, precision, version, est_cls):
-    from amber_b200 import estimate, Estimator
+    from amber_b200 import estimate
     return estimate(real, precision=precision, version=version)
 
 
